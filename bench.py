@@ -1,0 +1,415 @@
+"""Benchmark: one LJ snapshot through IFC3 assembly + mcc3 per step.
+
+Workload (the precision configuration): 256-atom FCC argon (4×4×4 cells,
+a = 5.2468 Å), positions displaced by i.i.d. N(0, 0.05²) Å (seeded),
+σ = 3.4 Å, ϵ = 0.24037 kcal/mol, r_cut = 8.5 Å, tol = 1e-12, m = 39.95 u;
+φ = eigenvectors of the dynamical matrix (FP32).  One step = dense FP64 IFC3
+assembly (+ASR, tol) with the fused mass-weighted split operand, then mcc3 over
+all 768 modes (three mode products), K3 in FP32.  Inputs are synthetic (seeded).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3|tf32x3|fp32]
+                    [--impl ours|reference]
+
+Prints one JSON line (rank 0).  Time-like metric: value = seconds per snapshot
+for the whole job (max over ranks of the device time ÷ all snapshots).  N > 1
+runs N independent replicas (one snapshot stream per GPU, no collective on the
+data path).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "forceconstants.jl_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "IFC3+mcc3 s/snapshot (256-atom LJ), split-BF16 vs FP32 GPU at ≤1e-5 rel err"
+UNIT = "s/snapshot"
+CELLS, A_LAT, STD, SEED = (4, 4, 4), 5.2468, 0.05, 1234
+SIGMA, EPS, R_CUT, TOL, MASS = 3.4, 0.24037, 8.5, 1e-12, 39.95
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return FALLBACK_PEAKS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks / throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(fcb, device):
+    import torch
+    s = fcb.displaced(fcb.FCC(A_LAT, "Ar", CELLS), STD, SEED)
+    pot = fcb.LJ(SIGMA, EPS, R_CUT)
+    calc = fcb.AnalyticalCalculator(TOL, R_CUT)
+    dyn = fcb.dynamical_matrix(s, pot, calc)               # on the GPU (fcb200_second_order_lj)
+    _, phi = fcb.get_modes(dyn)                             # host LAPACK, as the reference (dynmat.jl:125)
+    phi32 = np.asfortranarray(phi.astype(np.float32))
+    return s, pot, calc, phi32
+
+
+def julia_tensor(shape, dtype, device):
+    from fcb200.arrays import julia_empty
+    return julia_empty(shape, dtype, device)
+
+
+def fp64_reference_k3(psi64_dev, masses, phi32):
+    """FP64 K3 of the same inputs on the GPU (torch float64 tensordot), used
+    only to report the error of the timed path; not part of the timed region."""
+    import torch
+    n = psi64_dev.shape[0]
+    m = torch.from_numpy(np.repeat(masses, 3)).cuda()
+    w = torch.rsqrt(m[:, None, None] * m[None, :, None] * m[None, None, :])
+    mw = (psi64_dev * w).contiguous()                       # [i,j,k] semantics preserved
+    phi = torch.from_numpy(np.ascontiguousarray(phi32.astype(np.float64))).cuda()
+    k1 = torch.tensordot(phi, mw, dims=([0], [0]))          # [n, j, k]
+    del mw
+    k2 = torch.tensordot(k1, phi, dims=([1], [0]))          # [n, k, m]
+    del k1
+    k3 = torch.tensordot(k2, phi, dims=([1], [0]))          # [n, m, l]
+    return k3
+
+
+def err_vs(k3_dev, ref):
+    import torch
+    d = k3_dev.to(torch.float64) - ref
+    scale = ref.abs().max()
+    return {"max_rel": float(d.abs().max() / scale),
+            "rms_rel": float(torch.sqrt((d * d).mean()) / torch.sqrt((ref * ref).mean()))}
+
+
+def cpu_baseline(threads=None):
+    """The oracle (CPU restatement of the reference path) on the host cores:
+    full 256-atom third_order (all threads) + serial mass weighting + FP32 cast
+    measured; the FP64 mcc3 timed on 1/16 of mode product 1 and scaled by flops."""
+    from oracle import oracle as O
+    import fcb200 as fcb
+    if threads:
+        O.set_threads(threads)
+    s = fcb.displaced(fcb.FCC(A_LAT, "Ar", CELLS), STD, SEED)
+    n = 3 * s.n_atoms
+    t0 = time.perf_counter()
+    psi = O.third_order_lj(s.positions, s.box_sizes, SIGMA, EPS, R_CUT, TOL)
+    t1 = time.perf_counter()
+    O.mass_weight_third_order(psi, s.masses)
+    t2 = time.perf_counter()
+    f32 = np.empty(n ** 3, np.float32)
+    O.lib().oracle_cast_f32(O._pd(psi.reshape(-1, order="F")), f32.ctypes.data_as(O._PF), n ** 3)
+    t3 = time.perf_counter()
+    phi = np.linalg.qr(np.random.default_rng(0).normal(size=(n, n)))[0]
+    a = psi.reshape(n, n * n, order="F")
+    frac = 16
+    t4 = time.perf_counter()
+    _ = phi.T @ a[:, : n * n // frac]
+    t5 = time.perf_counter()
+    mcc3_est = (t5 - t4) * frac * 3
+    total = (t1 - t0) + (t2 - t1) + (t3 - t2) + mcc3_est
+    return {"value": total, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": (f"oracle on the full 256-atom cell: third_order {t1 - t0:.2f}s ({O.num_threads()} threads) + "
+                       f"serial mass_weight {t2 - t1:.2f}s + cast {t3 - t2:.2f}s measured; FP64 mcc3 "
+                       f"{mcc3_est:.2f}s scaled from 1/{frac} of mode product 1 (numpy BLAS) x3 products")}
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference path restated — CPU third_order (oracle,
+    all host threads) + serial mass weighting + Float32 cast, then the blocked
+    mcc3 (block_size 256, 27 blocks, D2H per block) with cuBLAS FP32 (TF32 off)
+    standing in for CUDA.jl + cuTENSOR on the same GPU."""
+    if rank != 0:
+        return
+    import torch
+    from oracle import oracle as O
+    import fcb200 as fcb
+    torch.backends.cuda.matmul.allow_tf32 = False
+    s = fcb.displaced(fcb.FCC(A_LAT, "Ar", CELLS), STD, SEED)
+    n = 3 * s.n_atoms
+    ifc2 = O.second_order_lj(s.positions, s.box_sizes, SIGMA, EPS, R_CUT, TOL)
+    _, phi = O.get_modes(O.dynamical_matrix(ifc2, s.masses))
+    phi_d = torch.from_numpy(np.ascontiguousarray(phi.astype(np.float32))).cuda()
+    b = 256
+    k3_host = torch.empty(n ** 3, dtype=torch.float32).numpy()
+
+    def step():
+        psi = O.third_order_lj(s.positions, s.box_sizes, SIGMA, EPS, R_CUT, TOL)
+        O.mass_weight_third_order(psi, s.masses)
+        psi32 = psi.astype(np.float32, order="F")
+        del psi
+        # [i,j,k] semantics: a Fortran array viewed through numpy keeps indices.
+        dpsi = torch.from_numpy(np.ascontiguousarray(psi32.transpose(2, 1, 0))).cuda()  # [k,j,i] row-major
+        del psi32
+        out = k3_host.reshape((n, n, n), order="F")
+        # mcc.jl:102-114: every block contracts all of Ψ with column-sliced φ
+        # (mcc3_blocked!, mcc.jl:129-131), then copies the block to the host.
+        for a0 in range(0, n, b):
+            for b0 in range(0, n, b):
+                for c0 in range(0, n, b):
+                    k1 = torch.matmul(dpsi, phi_d[:, a0:a0 + b])                  # [k,j,p]
+                    k2 = torch.einsum("kjp,jq->kpq", k1, phi_d[:, b0:b0 + b])     # [k,p,q]
+                    del k1
+                    k3 = torch.einsum("kpq,kr->pqr", k2, phi_d[:, c0:c0 + b])     # [p,q,r]
+                    out[a0:a0 + b, b0:b0 + b, c0:c0 + b] = k3.cpu().numpy()
+        torch.cuda.synchronize()
+
+    steps, warm = min(args.steps, 3), min(args.warmup, 1)
+    for _ in range(warm):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    dt = (time.perf_counter() - t0) / steps
+    line = {"metric": METRIC, "value": dt, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
+            "ms_per_step": dt * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "LJ FCC 4x4x4 (256 atoms, n=768), displaced std 0.05 A seed 1234; "
+                                   "CPU third_order+mass_weight+cast, then blocked FP32 mcc3 (block 256)",
+                       "mcc3_standin": "torch/cuBLAS FP32, TF32 off, 27 blocks with D2H per block"},
+            "cpu_baseline": {"value": dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+                             "sample": "one full snapshot per step (oracle CPU assembly + cuBLAS FP32 blocked mcc3)"},
+            "e2e": {"value": dt, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32x3", "fp32"])
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
+    ap.add_argument("--skip-e2e", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+
+    import fcb200 as fcb
+    from fcb200 import _lib
+    L = _lib.lib()
+    dev = f"cuda:{local}"
+    s, pot, calc, phi32 = build_workload(fcb, dev)
+    n = 3 * s.n_atoms
+    stream = torch.cuda.current_stream()
+    sp = int(stream.cuda_stream)
+    h = _lib.handle(local)
+    d_pos = torch.from_numpy(s.positions).to(dev)
+    d_box = torch.from_numpy(s.box_sizes).to(dev)
+    d_m = torch.from_numpy(s.masses).to(dev)
+    d_phi = torch.from_numpy(phi32).to(dev)
+    psi64 = julia_tensor((n, n, n), np.float64, dev)
+    k3 = julia_tensor((n, n, n), np.float32, dev)
+    prec = _lib.PRECISIONS[args.precision]
+
+    def step(precision=prec, k3_ptr=None, phi_ptr=None, pos_ptr=None):
+        _lib.check(L.fcb200_snapshot_lj(
+            h, pos_ptr or int(d_pos.data_ptr()), s.n_atoms, int(d_box.data_ptr()), SIGMA, EPS, R_CUT, TOL,
+            int(d_m.data_ptr()), phi_ptr or int(d_phi.data_ptr()), 0, n, precision, int(psi64.data_ptr()),
+            k3_ptr or int(k3.data_ptr()), sp))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = (ms / 1e3) / (args.steps * world)
+
+    # ---- per-phase device times (profiled pass, same stream, outside the timed region)
+    _lib.check(L.fcb200_set_profiling(h, 1))
+    reps = 3
+    acc = np.zeros(6)
+    for _ in range(reps):
+        step()
+        out = (ctypes.c_double * 6)()
+        _lib.check(L.fcb200_phase_times(h, out, 6))
+        acc += np.array(out[:])
+    _lib.check(L.fcb200_set_profiling(h, 0))
+    phases = acc / reps
+    names = ["pair_tables", "ifc3_dense_write", "phi_split", "mode_product_1", "mode_product_2", "mode_product_3"]
+    phase_ms = {k: round(float(v), 4) for k, v in zip(names, phases)}
+
+    peaks, peak_src = load_peaks()
+    split = 3 if args.precision != "fp32" else 1
+    mp_ms = float(np.mean(phases[3:6]))
+    flops_launch = 2.0 * n * n * n * n * split     # R·K·M = n⁴ per product at full modes
+    if args.precision == "fp32":
+        roof = {"bound": "fp32-simt", "achieved": flops_launch / (mp_ms * 1e-3) / 1e12, "peak": None,
+                "unit": "TFLOP/s", "frac": None, "traffic": None}
+    else:
+        pk = peaks["bf16_tflops_sustained"] if args.precision == "bf16x3" else None
+        ach = flops_launch / (mp_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": round(ach, 2), "peak": pk, "unit": "TFLOP/s",
+                "frac": round(ach / pk, 4) if pk else None, "traffic": None,
+                "kernel": f"mode_product_tc_kernel ({args.precision}), 3 launches/step",
+                "flops_per_launch": flops_launch, "avg_launch_ms": round(mp_ms, 4),
+                "peak_source": f"{peak_src} bf16_tflops_sustained (tensor flops executed = 3x useful for the split)"}
+    asm_bytes = 8.0 * n ** 3 + (4.0 if args.precision != "fp32" else 4.0) * n ** 3
+    asm_ms = float(phases[1])
+    roof_asm = {"bound": "hbm", "achieved": round(asm_bytes / (asm_ms * 1e-3) / 1e9, 1), "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": round(asm_bytes / (asm_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4),
+                "traffic": None, "kernel": "ifc3_dense_kernel", "bytes_per_launch": asm_bytes,
+                "avg_launch_ms": round(asm_ms, 4)}
+
+    # ---- accuracy of the timed path vs FP64 (outside timing)
+    torch.cuda.synchronize()
+    ref = fp64_reference_k3(psi64, s.masses, phi32)
+    acc_err = {args.precision: err_vs(k3, ref)}
+    # FP32 GPU form for the "split-BF16 vs FP32 GPU" comparison
+    fp32_info = None
+    if args.precision != "fp32":
+        k3f = julia_tensor((n, n, n), np.float32, dev)
+        step(precision=_lib.FCB_MCC3_FP32, k3_ptr=int(k3f.data_ptr()))
+        torch.cuda.synchronize()
+        acc_err["fp32"] = err_vs(k3f, ref)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        nf = 3
+        for _ in range(nf):
+            step(precision=_lib.FCB_MCC3_FP32, k3_ptr=int(k3f.data_ptr()))
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fp32_s = f0.elapsed_time(f1) / nf / 1e3
+        fp32_info = {"s_per_snapshot": fp32_s, "speedup_split_vs_fp32": fp32_s / (ms_per_step / 1e3)}
+        del k3f
+    del ref
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if not args.skip_e2e:
+        pos_h = np.ascontiguousarray(s.positions)
+        phi_h = torch.from_numpy(phi32.reshape(-1, order="F").copy()).pin_memory()
+        k3_h = torch.empty(n ** 3, dtype=torch.float32).pin_memory()
+        ne = max(3, min(args.steps, 5))
+        step(k3_ptr=int(k3_h.data_ptr()), phi_ptr=int(phi_h.data_ptr()), pos_ptr=pos_h.ctypes.data)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            step(k3_ptr=int(k3_h.data_ptr()), phi_ptr=int(phi_h.data_ptr()), pos_ptr=pos_h.ctypes.data)
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t0) / ne
+        e2e = {"value": e2e_s / world if world > 1 else e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(pos_h.nbytes + phi_h.numel() * 4),
+               "d2h_bytes_per_step": int(k3_h.numel() * 4),
+               "note": "fcb200_snapshot_lj with host positions, pinned host phi and pinned host K3; "
+                       "FP64 Psi stays in device memory"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu = cpu_baseline()
+
+    kernels_per_step = 7 if args.precision != "fp32" else 6
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64+" + args.precision, "data": "synthetic",
+        "config": {"workload": "LJ FCC 4x4x4 (256 atoms, n=768), displaced std 0.05 A (seed 1234), "
+                               "IFC3 FP64 + mass-weighted split operand, mcc3 all 768 modes",
+                   "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "l2": "working set > L2 (Psi64 3.6 GB, intermediates 1.8 GB each); no flush"},
+        "roofline": roof, "roofline_assembly": roof_asm, "phase_ms": phase_ms,
+        "error_vs_fp64": acc_err, "fp32_gpu": fp32_info, "clocks": clk, "e2e": e2e,
+        "cpu_baseline": cpu, "gpu_launches": kernels_per_step * args.steps,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,551 @@
+// extern "C" entry points of libfcb200 (declared in include/fcb200.h).
+//
+// The host side here only validates arguments, stages host buffers, sizes the
+// handle's scratch and sequences kernel launches on the caller's stream; all
+// arithmetic runs in the kernels of lj_assembly.cu, mode_product_*.cu and
+// mcc3.cu.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "fcb200_internal.cuh"
+
+namespace fcb {
+
+namespace {
+thread_local std::string t_msg = "no error";
+thread_local int t_code = FCB_OK;
+}  // namespace
+
+int set_error(int code, const std::string& msg) {
+    t_code = code;
+    t_msg = msg;
+    return code;
+}
+
+int cuda_error(cudaError_t e, const char* what) {
+    return set_error(e == cudaErrorMemoryAllocation ? FCB_ERR_OOM : FCB_ERR_CUDA,
+                     std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int Buf::ensure(size_t need) {
+    if (need <= bytes && p != nullptr) return FCB_OK;
+    release();
+    if (need == 0) return FCB_OK;
+    cudaError_t e = cudaMalloc(&p, need);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        bytes = 0;
+        cudaGetLastError();
+        return set_error(FCB_ERR_OOM, "device allocation of " + std::to_string(need) + " bytes refused: " +
+                                          cudaGetErrorString(e));
+    }
+    bytes = need;
+    return FCB_OK;
+}
+
+void Buf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+bool is_device_ptr(const void* ptr) {
+    if (ptr == nullptr) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+namespace {
+
+// Device view of a caller buffer: the pointer itself when it is device memory,
+// otherwise a handle scratch buffer (filled from the host when `upload`).
+template <class T>
+int device_view(Buf& scratch, const T* user, size_t count, bool upload, cudaStream_t s, T** out) {
+    if (user == nullptr) {
+        *out = nullptr;
+        return FCB_OK;
+    }
+    if (is_device_ptr(user)) {
+        *out = const_cast<T*>(user);
+        return FCB_OK;
+    }
+    FCB_TRY(scratch.ensure(sizeof(T) * count));
+    if (upload) FCB_CUDA(cudaMemcpyAsync(scratch.p, user, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+    *out = scratch.as<T>();
+    return FCB_OK;
+}
+
+int check_status(fcb200_context* h, cudaStream_t s) {
+    FCB_CUDA(cudaStreamSynchronize(s));
+    int st = 0;
+    FCB_CUDA(cudaMemcpy(&st, h->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != DEV_OK) {
+        int zero = 0;
+        cudaMemcpy(h->d_status, &zero, sizeof(int), cudaMemcpyHostToDevice);
+        return set_error(FCB_ERR_TIMEOUT, "a bounded device-side wait gave up (code " + std::to_string(st) +
+                                              "); the kernel returned early and its output is invalid");
+    }
+    return FCB_OK;
+}
+
+int esz_of(int kind) { return kind == 1 ? 2 : 4; }
+
+int validate_lj(const double* pos, int64_t N, const double* box, double r_cut, const double* masses,
+                bool need_masses) {
+    if (pos == nullptr || box == nullptr) return set_error(FCB_ERR_ARG, "pos and box must not be NULL");
+    if (N < 1) return set_error(FCB_ERR_ARG, "n_atoms must be >= 1");
+    if (N > 4096) return set_error(FCB_ERR_ARG, "n_atoms > 4096 (dense n³ tensor would exceed device memory)");
+    if (need_masses && masses == nullptr) return set_error(FCB_ERR_ARG, "masses are required for mass weighting");
+    if (!(r_cut > 0.0)) return set_error(FCB_ERR_ARG, "r_cut must be positive");
+    return FCB_OK;
+}
+
+int check_cutoff(const double* box_host) {
+    for (int d = 0; d < 3; ++d)
+        if (!(box_host[d] > 0.0)) return set_error(FCB_ERR_ARG, "box lengths must be positive");
+    return FCB_OK;
+}
+
+// Reads the 3 box lengths to the host (the r_cut < L check of
+// third_order_analytical.jl:7 is a host-side status, not a device assert).
+int box_to_host(const double* box, double out[3]) {
+    if (is_device_ptr(box)) {
+        FCB_CUDA(cudaMemcpy(out, box, 3 * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+        memcpy(out, box, 3 * sizeof(double));
+    }
+    return FCB_OK;
+}
+
+struct Mcc3Operand {
+    const float* f32 = nullptr;  // FP32 Ψ with lda = n
+    const void* hi = nullptr;    // split planes with lda = n_pad
+    const void* lo = nullptr;
+};
+
+// P1..P3 on device buffers.  `emit` receives each finished slab of the last
+// mode axis when slab > 0 (used by the blocked / host-output forms).
+int run_mcc3(fcb200_context* h, int precision, const Mcc3Operand& psi, const float* d_phi, int64_t n,
+             int64_t n_lo, int64_t n_hi, int64_t m_lo, int64_t m_hi, int64_t l_lo, int64_t l_hi, float* d_k3,
+             cudaStream_t s) {
+    const int64_t Mn = n_hi - n_lo, Mm = m_hi - m_lo, Ml = l_hi - l_lo;
+    if (precision == FCB_MCC3_FP32) {
+        FCB_TRY(h->u1_f32.ensure(sizeof(float) * n * n * Mn));
+        FCB_TRY(h->u2_f32.ensure(sizeof(float) * n * Mn * Mm));
+        phase_mark(h, s, 3);
+        ModeProduct p1{n * n, n, Mn, n, n, n, n, n * n};
+        FCB_TRY(mode_product_f32(psi.f32, d_phi + n * n_lo, h->u1_f32.as<float>(), p1, s));
+        phase_mark(h, s, 4);
+        ModeProduct p2{n * Mn, n, Mm, n, n, n, n, n * Mn};
+        FCB_TRY(mode_product_f32(h->u1_f32.as<float>(), d_phi + n * m_lo, h->u2_f32.as<float>(), p2, s));
+        phase_mark(h, s, 5);
+        ModeProduct p3{Mn * Mm, n, Ml, n, n, Mn * Mm, Mn * Mm, Mn * Mm};
+        FCB_TRY(mode_product_f32(h->u2_f32.as<float>(), d_phi + n * l_lo, d_k3, p3, s));
+        phase_mark(h, s, 6);
+        return FCB_OK;
+    }
+    const int kind = precision == FCB_MCC3_BF16X3 ? 1 : 2;
+    const int64_t np = pad_for(kind, n);
+    const size_t esz = esz_of(kind);
+    // φ planes for all n columns: [mode][n_pad]
+    FCB_TRY(h->phi_hi.ensure(esz * np * n));
+    FCB_TRY(h->phi_lo.ensure(esz * np * n));
+    FCB_TRY(split_operand(d_phi, n, n, n, h->phi_hi.p, h->phi_lo.p, np, kind, s));
+    phase_mark(h, s, 3);
+    FCB_TRY(h->u1_hi.ensure(esz * np * n * Mn));
+    FCB_TRY(h->u1_lo.ensure(esz * np * n * Mn));
+    FCB_TRY(h->u2_hi.ensure(esz * np * Mn * Mm));
+    FCB_TRY(h->u2_lo.ensure(esz * np * Mn * Mm));
+    auto plane = [&](const Buf& b, int64_t mode) {
+        return static_cast<const void*>(static_cast<const uint8_t*>(b.p) + esz * np * mode);
+    };
+    ModeProduct p1{n * n, n, Mn, np, np, n, np, np * n};
+    FCB_TRY(mode_product_tc(h, kind, psi.hi, psi.lo, plane(h->phi_hi, n_lo), plane(h->phi_lo, n_lo), h->u1_hi.p,
+                            h->u1_lo.p, kind, p1, s));
+    phase_mark(h, s, 4);
+    ModeProduct p2{n * Mn, n, Mm, np, np, n, np, np * Mn};
+    FCB_TRY(mode_product_tc(h, kind, h->u1_hi.p, h->u1_lo.p, plane(h->phi_hi, m_lo), plane(h->phi_lo, m_lo),
+                            h->u2_hi.p, h->u2_lo.p, kind, p2, s));
+    phase_mark(h, s, 5);
+    ModeProduct p3{Mn * Mm, n, Ml, np, np, Mn * Mm, Mn * Mm, Mn * Mm};
+    FCB_TRY(mode_product_tc(h, kind, h->u2_hi.p, h->u2_lo.p, plane(h->phi_hi, l_lo), plane(h->phi_lo, l_lo), d_k3,
+                            nullptr, 0, p3, s));
+    phase_mark(h, s, 6);
+    return FCB_OK;
+}
+
+int check_precision(int precision) {
+    if (precision != FCB_MCC3_FP32 && precision != FCB_MCC3_BF16X3 && precision != FCB_MCC3_TF32X3)
+        return set_error(FCB_ERR_ARG, "unknown mcc3 precision mode");
+    return FCB_OK;
+}
+
+// Stage the mass-weighted Ψ operand for a given precision from an FP32 Ψ.
+int psi_operand_from_f32(fcb200_context* h, int precision, const float* d_psi, int64_t n, cudaStream_t s,
+                         Mcc3Operand* op) {
+    if (precision == FCB_MCC3_FP32) {
+        op->f32 = d_psi;
+        return FCB_OK;
+    }
+    const int kind = precision == FCB_MCC3_BF16X3 ? 1 : 2;
+    const int64_t np = pad_for(kind, n);
+    FCB_TRY(h->psi_hi.ensure((size_t)esz_of(kind) * np * n * n));
+    FCB_TRY(h->psi_lo.ensure((size_t)esz_of(kind) * np * n * n));
+    FCB_TRY(split_operand(d_psi, n * n, n, n, h->psi_hi.p, h->psi_lo.p, np, kind, s));
+    op->hi = h->psi_hi.p;
+    op->lo = h->psi_lo.p;
+    return FCB_OK;
+}
+
+}  // namespace
+}  // namespace fcb
+
+using namespace fcb;
+
+extern "C" {
+
+int fcb200_version(void) { return 100; }
+
+int fcb200_last_error(char* buf, size_t len) {
+    if (buf && len) {
+        strncpy(buf, t_msg.c_str(), len - 1);
+        buf[len - 1] = '\0';
+    }
+    return t_code;
+}
+
+int fcb200_create(fcb200_handle* out, int device) {
+    if (!out) return set_error(FCB_ERR_ARG, "out must not be NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return set_error(FCB_ERR_UNSUPPORTED, "no CUDA device available");
+    }
+    if (device < 0 || device >= count) return set_error(FCB_ERR_ARG, "device index out of range");
+    FCB_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    FCB_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+        return set_error(FCB_ERR_UNSUPPORTED, std::string("fcb200 requires an sm_100 (B200) device, found ") + prop.name);
+    auto* h = new fcb200_context();
+    h->device = device;
+    h->sm_count = prop.multiProcessorCount;
+    if (cudaMalloc(&h->d_status, sizeof(int)) != cudaSuccess) {
+        delete h;
+        return set_error(FCB_ERR_OOM, "status word allocation failed");
+    }
+    cudaMemset(h->d_status, 0, sizeof(int));
+    cudaStreamCreateWithFlags(&h->aux_stream, cudaStreamNonBlocking);
+    for (auto& ev : h->ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    *out = h;
+    return FCB_OK;
+}
+
+int fcb200_trim(fcb200_handle h) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    cudaSetDevice(h->device);
+    Buf* bufs[] = {&h->pos, &h->box, &h->masses, &h->pair_t, &h->pair_flag, &h->self_t, &h->psi_stage,
+                   &h->phi_f32, &h->phi_hi, &h->phi_lo, &h->psi_hi, &h->psi_lo, &h->u1_hi, &h->u1_lo,
+                   &h->u2_hi, &h->u2_lo, &h->u1_f32, &h->u2_f32, &h->psi_f32, &h->k3_stage[0],
+                   &h->k3_stage[1], &h->ifc2};
+    for (Buf* b : bufs) b->release();
+    return FCB_OK;
+}
+
+int fcb200_destroy(fcb200_handle h) {
+    if (!h) return FCB_OK;
+    cudaSetDevice(h->device);
+    fcb200_trim(h);
+    if (h->d_status) cudaFree(h->d_status);
+    if (h->aux_stream) cudaStreamDestroy(h->aux_stream);
+    for (auto& e : h->pev)
+        if (e) cudaEventDestroy(e);
+    for (auto& ev : h->ev)
+        if (ev) cudaEventDestroy(ev);
+    delete h;
+    return FCB_OK;
+}
+
+int fcb200_synchronize(fcb200_handle h, void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    return check_status(h, static_cast<cudaStream_t>(stream));
+}
+
+int fcb200_set_profiling(fcb200_handle h, int enable) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    cudaSetDevice(h->device);
+    if (enable && !h->pev[0])
+        for (auto& e : h->pev) FCB_CUDA(cudaEventCreate(&e));
+    h->profiling = enable != 0;
+    return FCB_OK;
+}
+
+int fcb200_phase_times(fcb200_handle h, double* ms, int max_phases) {
+    if (!h || !ms) return set_error(FCB_ERR_ARG, "NULL argument");
+    cudaSetDevice(h->device);
+    int k = 0;
+    for (int i = 0; i + 1 < fcb200_context::kMarks && k < max_phases; ++i, ++k) {
+        ms[k] = -1.0;
+        if (h->profiling && h->marked[i] && h->marked[i + 1]) {
+            float t = 0.f;
+            FCB_CUDA(cudaEventSynchronize(h->pev[i + 1]));
+            FCB_CUDA(cudaEventElapsedTime(&t, h->pev[i], h->pev[i + 1]));
+            ms[k] = t;
+        }
+    }
+    return FCB_OK;
+}
+
+int fcb200_third_order_lj(fcb200_handle h, const double* pos, int64_t N, const double* box, double sigma,
+                          double eps, double r_cut, double tol, const double* masses, double* psi_out,
+                          float* psi32_mw_out, int flags, void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    const bool weighted = (flags & FCB_PSI_MASS_WEIGHTED) != 0;
+    FCB_TRY(validate_lj(pos, N, box, r_cut, masses, weighted || psi32_mw_out != nullptr));
+    double bh[3];
+    FCB_TRY(box_to_host(box, bh));
+    FCB_TRY(check_cutoff(bh));
+    for (int d = 0; d < 3; ++d)
+        if (!(r_cut < bh[d])) return set_error(FCB_ERR_CUTOFF, "Cutoff larger than L/2 (r_cut must be < box length)");
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t n = 3 * N;
+    double *d_pos, *d_box, *d_m;
+    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
+    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
+    FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
+    FCB_TRY(lj_pair_tables(h, d_pos, N, d_box, sigma, eps, r_cut, s));
+    AssemblyOut out;
+    const bool host64 = psi_out && !is_device_ptr(psi_out);
+    const bool host32 = psi32_mw_out && !is_device_ptr(psi32_mw_out);
+    if (host64 && host32) {
+        FCB_TRY(h->psi_stage.ensure(sizeof(double) * n * n * n));
+        FCB_TRY(h->psi_f32.ensure(sizeof(float) * n * n * n));
+    } else if (host64) {
+        FCB_TRY(h->psi_stage.ensure(sizeof(double) * n * n * n));
+    } else if (host32) {
+        FCB_TRY(h->psi_f32.ensure(sizeof(float) * n * n * n));
+    }
+    out.psi64 = psi_out ? (host64 ? h->psi_stage.as<double>() : psi_out) : nullptr;
+    out.psi64_weighted = weighted;
+    out.psi32 = psi32_mw_out ? (host32 ? h->psi_f32.as<float>() : psi32_mw_out) : nullptr;
+    FCB_TRY(ifc3_dense_write(h, N, tol, d_m, out, s));
+    if (host64) FCB_CUDA(cudaMemcpyAsync(psi_out, out.psi64, sizeof(double) * n * n * n, cudaMemcpyDeviceToHost, s));
+    if (host32)
+        FCB_CUDA(cudaMemcpyAsync(psi32_mw_out, out.psi32, sizeof(float) * n * n * n, cudaMemcpyDeviceToHost, s));
+    if (host64 || host32 || !is_device_ptr(pos) || !is_device_ptr(box) || (masses && !is_device_ptr(masses)))
+        return check_status(h, s);
+    return FCB_OK;
+}
+
+int fcb200_mass_weight3(fcb200_handle h, double* psi, const double* masses, int64_t N, void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    if (!psi || !masses) return set_error(FCB_ERR_ARG, "psi and masses must not be NULL");
+    if (N < 1) return set_error(FCB_ERR_ARG, "n_atoms must be >= 1");
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t n = 3 * N;
+    double* d_m;
+    FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
+    const bool host = !is_device_ptr(psi);
+    double* d_psi = psi;
+    if (host) {
+        FCB_TRY(h->psi_stage.ensure(sizeof(double) * n * n * n));
+        d_psi = h->psi_stage.as<double>();
+        FCB_CUDA(cudaMemcpyAsync(d_psi, psi, sizeof(double) * n * n * n, cudaMemcpyHostToDevice, s));
+    }
+    FCB_TRY(mass_weight3_launch(d_psi, d_m, N, s));
+    if (host) {
+        FCB_CUDA(cudaMemcpyAsync(psi, d_psi, sizeof(double) * n * n * n, cudaMemcpyDeviceToHost, s));
+        return check_status(h, s);
+    }
+    return FCB_OK;
+}
+
+int fcb200_second_order_lj(fcb200_handle h, const double* pos, int64_t N, const double* box, double sigma,
+                           double eps, double r_cut, double tol, const double* masses, double* ifc2_out,
+                           void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    FCB_TRY(validate_lj(pos, N, box, r_cut, masses, false));
+    if (!ifc2_out) return set_error(FCB_ERR_ARG, "ifc2_out must not be NULL");
+    double bh[3];
+    FCB_TRY(box_to_host(box, bh));
+    FCB_TRY(check_cutoff(bh));
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t n = 3 * N;
+    double *d_pos, *d_box, *d_m, *d_out;
+    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
+    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
+    FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
+    FCB_TRY(device_view(h->ifc2, (const double*)ifc2_out, n * n, false, s, &d_out));
+    FCB_TRY(lj_second_order_launch(h, d_pos, N, d_box, sigma, eps, r_cut, tol, d_m, d_out, s));
+    if (d_out != ifc2_out) {
+        FCB_CUDA(cudaMemcpyAsync(ifc2_out, d_out, sizeof(double) * n * n, cudaMemcpyDeviceToHost, s));
+        return check_status(h, s);
+    }
+    return FCB_OK;
+}
+
+static int mcc3_ranges_ok(int64_t n, int64_t a, int64_t b) { return 0 <= a && a < b && b <= n; }
+
+int fcb200_mcc3(fcb200_handle h, const float* psi, const float* phi, int64_t n, int64_t n_lo, int64_t n_hi,
+                int64_t m_lo, int64_t m_hi, int64_t l_lo, int64_t l_hi, int precision, float* k3_out,
+                void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    if (!psi || !phi || !k3_out) return set_error(FCB_ERR_ARG, "psi, phi and k3_out must not be NULL");
+    if (n < 1) return set_error(FCB_ERR_ARG, "n must be >= 1");
+    if (!mcc3_ranges_ok(n, n_lo, n_hi) || !mcc3_ranges_ok(n, m_lo, m_hi) || !mcc3_ranges_ok(n, l_lo, l_hi))
+        return set_error(FCB_ERR_ARG, "mode window outside [0, n)");
+    FCB_TRY(check_precision(precision));
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float *d_psi, *d_phi, *d_k3;
+    FCB_TRY(device_view(h->psi_f32, psi, (size_t)(n * n * n), true, s, &d_psi));
+    FCB_TRY(device_view(h->phi_f32, phi, (size_t)(n * n), true, s, &d_phi));
+    const size_t k3n = (size_t)((n_hi - n_lo) * (m_hi - m_lo) * (l_hi - l_lo));
+    FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, k3n, false, s, &d_k3));
+    Mcc3Operand op;
+    FCB_TRY(psi_operand_from_f32(h, precision, d_psi, n, s, &op));
+    FCB_TRY(run_mcc3(h, precision, op, d_phi, n, n_lo, n_hi, m_lo, m_hi, l_lo, l_hi, d_k3, s));
+    const bool host_io = d_k3 != k3_out || d_psi != psi || d_phi != phi;
+    if (d_k3 != k3_out) FCB_CUDA(cudaMemcpyAsync(k3_out, d_k3, sizeof(float) * k3n, cudaMemcpyDeviceToHost, s));
+    if (host_io) return check_status(h, s);
+    return FCB_OK;
+}
+
+int fcb200_mcc3_blocked(fcb200_handle h, const float* psi, const float* phi, int64_t n, int64_t block_size,
+                        int precision, float* k3_out, void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    if (!psi || !phi || !k3_out) return set_error(FCB_ERR_ARG, "psi, phi and k3_out must not be NULL");
+    if (n < 1) return set_error(FCB_ERR_ARG, "n must be >= 1");
+    if (block_size <= 0 || n % block_size != 0)
+        return set_error(FCB_ERR_BLOCK, "size(phi,1) must be a multiple of block_size (mcc.jl:91)");
+    FCB_TRY(check_precision(precision));
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float *d_psi, *d_phi;
+    FCB_TRY(device_view(h->psi_f32, psi, (size_t)(n * n * n), true, s, &d_psi));
+    FCB_TRY(device_view(h->phi_f32, phi, (size_t)(n * n), true, s, &d_phi));
+    Mcc3Operand op;
+    FCB_TRY(psi_operand_from_f32(h, precision, d_psi, n, s, &op));
+    const bool host_out = !is_device_ptr(k3_out);
+    const int64_t slab = n * n * block_size;  // floats per slab of the last mode axis
+    if (!host_out) {
+        FCB_TRY(run_mcc3(h, precision, op, d_phi, n, 0, n, 0, n, 0, n, k3_out, s));
+    } else {
+        // P1 and P2 once, then P3 slab by slab; each slab is copied back on the
+        // aux stream while the next one computes.
+        FCB_TRY(h->k3_stage[0].ensure(sizeof(float) * slab));
+        FCB_TRY(h->k3_stage[1].ensure(sizeof(float) * slab));
+        const int64_t nb = n / block_size;
+        for (int64_t b = 0; b < nb; ++b) {
+            const int slot = (int)(b & 1);
+            if (b >= 2) FCB_CUDA(cudaStreamWaitEvent(s, h->ev[slot], 0));  // slot's previous copy done
+            float* d_slab = h->k3_stage[slot].as<float>();
+            if (b == 0) {
+                FCB_TRY(run_mcc3(h, precision, op, d_phi, n, 0, n, 0, n, 0, block_size, d_slab, s));
+            } else {
+                // Only P3 for the remaining slabs: U2 is already resident.
+                const int64_t l0 = b * block_size;
+                if (precision == FCB_MCC3_FP32) {
+                    ModeProduct p3{n * n, n, block_size, n, n, n * n, n * n, n * n};
+                    FCB_TRY(mode_product_f32(h->u2_f32.as<float>(), d_phi + n * l0, d_slab, p3, s));
+                } else {
+                    const int kind = precision == FCB_MCC3_BF16X3 ? 1 : 2;
+                    const int64_t np = pad_for(kind, n);
+                    const size_t esz = esz_of(kind);
+                    ModeProduct p3{n * n, n, block_size, np, np, n * n, n * n, n * n};
+                    FCB_TRY(mode_product_tc(h, kind, h->u2_hi.p, h->u2_lo.p,
+                                            static_cast<uint8_t*>(h->phi_hi.p) + esz * np * l0,
+                                            static_cast<uint8_t*>(h->phi_lo.p) + esz * np * l0, d_slab, nullptr, 0,
+                                            p3, s));
+                }
+            }
+            FCB_CUDA(cudaEventRecord(h->ev[2], s));
+            FCB_CUDA(cudaStreamWaitEvent(h->aux_stream, h->ev[2], 0));
+            FCB_CUDA(cudaMemcpyAsync(k3_out + b * slab, d_slab, sizeof(float) * slab, cudaMemcpyDeviceToHost,
+                                     h->aux_stream));
+            FCB_CUDA(cudaEventRecord(h->ev[slot], h->aux_stream));
+        }
+        FCB_CUDA(cudaStreamSynchronize(h->aux_stream));
+    }
+    if (host_out || d_psi != psi || d_phi != phi) return check_status(h, s);
+    return FCB_OK;
+}
+
+int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t N, const double* box, double sigma, double eps,
+                       double r_cut, double tol, const double* masses, const float* phi, int64_t mode_lo,
+                       int64_t mode_hi, int precision, double* psi_out, float* k3_out, void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    FCB_TRY(validate_lj(pos, N, box, r_cut, masses, true));
+    if (!phi || !k3_out) return set_error(FCB_ERR_ARG, "phi and k3_out must not be NULL");
+    const int64_t n = 3 * N;
+    if (!mcc3_ranges_ok(n, mode_lo, mode_hi)) return set_error(FCB_ERR_ARG, "mode window outside [0, n)");
+    FCB_TRY(check_precision(precision));
+    double bh[3];
+    FCB_TRY(box_to_host(box, bh));
+    FCB_TRY(check_cutoff(bh));
+    for (int d = 0; d < 3; ++d)
+        if (!(r_cut < bh[d])) return set_error(FCB_ERR_CUTOFF, "Cutoff larger than L/2 (r_cut must be < box length)");
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double *d_pos, *d_box, *d_m;
+    float* d_phi;
+    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
+    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
+    FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
+    FCB_TRY(device_view(h->phi_f32, phi, (size_t)(n * n), true, s, &d_phi));
+    for (bool& m : h->marked) m = false;
+    phase_mark(h, s, 0);
+    FCB_TRY(lj_pair_tables(h, d_pos, N, d_box, sigma, eps, r_cut, s));
+    phase_mark(h, s, 1);
+    const bool host64 = psi_out && !is_device_ptr(psi_out);
+    if (host64) FCB_TRY(h->psi_stage.ensure(sizeof(double) * n * n * n));
+    AssemblyOut out;
+    out.psi64 = psi_out ? (host64 ? h->psi_stage.as<double>() : psi_out) : nullptr;
+    Mcc3Operand op;
+    if (precision == FCB_MCC3_FP32) {
+        FCB_TRY(h->psi_f32.ensure(sizeof(float) * n * n * n));
+        out.psi32 = h->psi_f32.as<float>();
+        op.f32 = out.psi32;
+    } else {
+        const int kind = precision == FCB_MCC3_BF16X3 ? 1 : 2;
+        const int64_t np = pad_for(kind, n);
+        FCB_TRY(h->psi_hi.ensure((size_t)esz_of(kind) * np * n * n));
+        FCB_TRY(h->psi_lo.ensure((size_t)esz_of(kind) * np * n * n));
+        out.split_hi = h->psi_hi.p;
+        out.split_lo = h->psi_lo.p;
+        out.split_kind = kind;
+        out.n_pad = np;
+        op.hi = out.split_hi;
+        op.lo = out.split_lo;
+    }
+    FCB_TRY(ifc3_dense_write(h, N, tol, d_m, out, s));
+    phase_mark(h, s, 2);
+    if (precision == FCB_MCC3_FP32) phase_mark(h, s, 3);  // no φ split phase
+    const int64_t M = mode_hi - mode_lo;
+    float* d_k3;
+    FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)(M * M * M), false, s, &d_k3));
+    FCB_TRY(run_mcc3(h, precision, op, d_phi, n, mode_lo, mode_hi, mode_lo, mode_hi, mode_lo, mode_hi, d_k3, s));
+    bool host = false;
+    if (host64) {
+        FCB_CUDA(cudaMemcpyAsync(psi_out, out.psi64, sizeof(double) * n * n * n, cudaMemcpyDeviceToHost, s));
+        host = true;
+    }
+    if (d_k3 != k3_out) {
+        FCB_CUDA(cudaMemcpyAsync(k3_out, d_k3, sizeof(float) * M * M * M, cudaMemcpyDeviceToHost, s));
+        host = true;
+    }
+    if (host || d_pos != pos || d_phi != phi) return check_status(h, s);
+    return FCB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,142 @@
+// Internal declarations shared by the fcb200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/fcb200.h"
+
+namespace fcb {
+
+// ---------------------------------------------------------------------------
+// Error reporting: each entry point returns a status; the message is kept per
+// thread for fcb200_last_error().
+// ---------------------------------------------------------------------------
+int set_error(int code, const std::string& msg);
+int cuda_error(cudaError_t e, const char* what);
+
+#define FCB_CUDA(call)                                                  \
+    do {                                                                \
+        cudaError_t e_ = (call);                                        \
+        if (e_ != cudaSuccess) return ::fcb::cuda_error(e_, #call);     \
+    } while (0)
+
+#define FCB_TRY(call)                    \
+    do {                                 \
+        int s_ = (call);                 \
+        if (s_ != FCB_OK) return s_;     \
+    } while (0)
+
+// Device-side status word codes (written by bounded waits).
+enum DeviceStatus : int {
+    DEV_OK = 0,
+    DEV_TIMEOUT_PRODUCER = 1,
+    DEV_TIMEOUT_MMA = 2,
+    DEV_TIMEOUT_EPILOGUE = 3,
+};
+
+// A device buffer cached in a handle and grown on demand.
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t need);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Split operand: two planes (hi, lo) of the same padded layout.
+struct SplitPlanes {
+    void* hi = nullptr;
+    void* lo = nullptr;
+};
+
+}  // namespace fcb
+
+struct fcb200_context {
+    int device = 0;
+    int sm_count = 0;
+    int* d_status = nullptr;        // device status word (bounded-wait failures)
+    // assembly scratch
+    fcb::Buf pos, box, masses;      // staged inputs
+    fcb::Buf pair_t, pair_flag;     // per ordered pair: 27 values of -ϕ₃ and a within-cut flag
+    fcb::Buf self_t;                // per atom: 27 ASR self values
+    fcb::Buf psi_stage;             // device copy of Ψ when the caller passes a host buffer
+    // mcc3 scratch
+    fcb::Buf phi_f32;               // staged φ (FP32)
+    fcb::Buf phi_hi, phi_lo;        // split φ (padded, [modes][n_pad])
+    fcb::Buf psi_hi, psi_lo;        // split Ψ
+    fcb::Buf u1_hi, u1_lo, u2_hi, u2_lo;  // split intermediates
+    fcb::Buf u1_f32, u2_f32;        // plain FP32 intermediates
+    fcb::Buf psi_f32;               // staged Ψ (FP32) for host inputs
+    fcb::Buf k3_stage[2];           // K3 staging slabs (device) for host outputs
+    fcb::Buf ifc2;                  // second-order scratch
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // Optional per-phase timing of fcb200_snapshot_lj (events on the caller's stream).
+    static constexpr int kMarks = 7;
+    bool profiling = false;
+    bool marked[kMarks] = {};
+    cudaEvent_t pev[kMarks] = {};
+};
+
+namespace fcb {
+
+bool is_device_ptr(const void* p);
+
+// Records phase mark i on stream s when profiling is enabled.
+inline void phase_mark(fcb200_context* h, cudaStream_t s, int i) {
+    if (h->profiling && i < fcb200_context::kMarks) {
+        cudaEventRecord(h->pev[i], s);
+        h->marked[i] = true;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// LJ assembly (lj_assembly.cu)
+// ---------------------------------------------------------------------------
+struct AssemblyOut {
+    double* psi64 = nullptr;        // n³ FP64 (column-major), may be null
+    bool psi64_weighted = false;    // write the mass-weighted value into psi64
+    float* psi32 = nullptr;         // n³ FP32 mass weighted (dense, stride n), may be null
+    void* split_hi = nullptr;       // split mass-weighted copy, padded stride n_pad
+    void* split_lo = nullptr;
+    int split_kind = 0;             // 0 none, 1 bf16 planes, 2 tf32 (fp32) planes
+    int64_t n_pad = 0;
+};
+
+int lj_pair_tables(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box,
+                   double sigma, double eps, double r_cut, cudaStream_t s);
+int ifc3_dense_write(fcb200_context* h, int64_t N, double tol, const double* d_masses,
+                     const AssemblyOut& out, cudaStream_t s);
+int mass_weight3_launch(double* d_psi, const double* d_masses, int64_t N, cudaStream_t s);
+int lj_second_order_launch(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box,
+                           double sigma, double eps, double r_cut, double tol,
+                           const double* d_masses, double* d_ifc2, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// mcc3 (mcc3.cu, mode_product_simt.cu, mode_product_tc.cu)
+// ---------------------------------------------------------------------------
+// One mode product  D[r,p] = Σ_a A[a + lda*r] * B[a + ldb*p],  r < R, p < M,
+// a < K; D stored at (r % F) + F_pad*(r / F) + ldd*p.
+struct ModeProduct {
+    int64_t R, K, M;
+    int64_t lda, ldb;
+    int64_t F, F_pad, ldd;
+};
+
+int mode_product_f32(const float* A, const float* B, float* D, const ModeProduct& mp,
+                     cudaStream_t s);
+// Split operands (hi/lo planes).  kind 1 = bf16, 2 = tf32 (fp32 planes).
+// out_kind: 0 = fp32 D (D_hi only), 1 = bf16 split D, 2 = tf32 split D.
+int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A_lo,
+                    const void* B_hi, const void* B_lo, void* D_hi, void* D_lo, int out_kind,
+                    const ModeProduct& mp, cudaStream_t s);
+int split_operand(const float* src, int64_t rows, int64_t cols, int64_t ld_src, void* hi, void* lo,
+                  int64_t ld_dst, int kind, cudaStream_t s);
+
+int pad_for(int kind, int64_t n);  // padded leading dimension for a split kind
+
+}  // namespace fcb

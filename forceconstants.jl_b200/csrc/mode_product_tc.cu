@@ -1,0 +1,449 @@
+// Split-precision mode product on the sm_100a tensor cores (tcgen05 + TMA + TMEM).
+//
+// One mode product of mcc3 (src/mcc.jl:35-47: K1[n,j,k] = Σ_i Ψ[i,j,k] φ[i,n],
+// and its two successors) is a GEMM
+//     D[r,p] = Σ_a A[a + lda*r] * B[a + ldb*p]        r < R, p < M, a < K
+// whose operands are both K-major (the contracted index is the contiguous one)
+// and whose output rows are contiguous, so the output of one product is
+// directly the K-major A operand of the next (the index order rotates
+// [i,j,k] → [j,k,n] → [k,n,m] → [n,m,l]).
+//
+// Each operand is held as two planes, hi and lo, with x ≈ hi + lo:
+//   kind 1: BF16 planes, tcgen05.mma.kind::f16   (BF16×3)
+//   kind 2: TF32 values in FP32 planes, tcgen05.mma.kind::tf32  (TF32×3)
+// and each K step issues hi·hi + hi·lo + lo·hi into one FP32 TMEM accumulator.
+//
+// Kernel structure (persistent, one CTA per SM, 192 threads):
+//   warp 0      TMA producer: 4 tiled loads per stage (A_hi, A_lo, B_hi, B_lo),
+//               128-byte swizzle, no multicast, completion on an mbarrier.
+//   warp 1      TMEM allocation (512 columns = two 128×256 FP32 accumulators)
+//               and the single MMA-issuing thread.
+//   warps 2..5  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM lanes
+//               32*(w%4)..+31), conversion to the output format (FP32, or the
+//               hi/lo planes of the next product) and coalesced stores.
+// Double-buffered accumulators let the epilogue of tile t overlap the MMAs of
+// tile t+1.  Every mbarrier wait is bounded by a wall-clock limit; on expiry
+// the CTA records an error in the device status word, drains its own copies
+// and MMAs in flight, frees TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "fcb200_internal.cuh"
+
+namespace fcb {
+namespace {
+
+constexpr int BM = 128;                    // tile rows (UMMA M)
+constexpr int BN_MAX = 256;                // tile modes (UMMA N upper bound)
+constexpr int ROW_BYTES = 128;             // one swizzle row of K per stage
+constexpr int STAGES = 2;
+constexpr int A_BYTES = BM * ROW_BYTES;    // 16 KB per plane
+constexpr int B_BYTES = BN_MAX * ROW_BYTES;  // 32 KB per plane
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+constexpr int TMEM_COLS = 2 * BN_MAX;
+constexpr int NUM_THREADS = 192;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr uint64_t TIMEOUT_NS = 2000000000ull;  // 2 s per wait
+
+struct TcParams {
+    int64_t R, K, M;
+    int64_t F, F_pad, ldd;
+    int bn, n_tiles, m_tiles, k_chunks, elems_per_row;
+    int out_kind;
+    void* d_hi;
+    void* d_lo;
+    int* status;
+};
+
+__device__ __forceinline__ uint32_t saddr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(saddr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait.  Returns false (after flagging the CTA and the device status
+// word) when the phase does not complete within TIMEOUT_NS, or when another
+// role of this CTA has already given up (unless `ignore_abort`).
+__device__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag, int* status, int code,
+                          bool ignore_abort = false) {
+    if (mbar_try(b, parity)) return true;
+    const uint64_t t0 = gtimer();
+    while (true) {
+        if (mbar_try(b, parity)) return true;
+        if (!ignore_abort && *abort_flag) return false;
+        if (gtimer() - t0 > TIMEOUT_NS) {
+            *abort_flag = 1;
+            atomicCAS(status, 0, code);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(saddr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(saddr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;             // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset
+    d |= (uint64_t)1 << 46;             // descriptor version for tcgen05
+    d |= (uint64_t)2 << 61;             // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor: FP32 accumulator, both operands K-major.
+template <int KIND>
+__device__ __forceinline__ uint32_t instr_desc(int m, int n) {
+    const uint32_t fmt = KIND == 1 ? 1u : 2u;  // BF16 : TF32
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+template <int KIND>
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    if constexpr (KIND == 1) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc));
+    }
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+          "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+          "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+          "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void store_out(const TcParams& p, int64_t off, float v) {
+    if (p.out_kind == 0) {
+        static_cast<float*>(p.d_hi)[off] = v;
+    } else if (p.out_kind == 1) {
+        __nv_bfloat16 h = __float2bfloat16_rn(v);
+        static_cast<__nv_bfloat16*>(p.d_hi)[off] = h;
+        static_cast<__nv_bfloat16*>(p.d_lo)[off] = __float2bfloat16_rn(v - __bfloat162float(h));
+    } else {
+        uint32_t hb;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(v));
+        const float h = __uint_as_float(hb);
+        static_cast<float*>(p.d_hi)[off] = h;
+        static_cast<float*>(p.d_lo)[off] = v - h;
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+    mode_product_tc_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant__ CUtensorMap mA_lo,
+                           const __grid_constant__ CUtensorMap mB_hi, const __grid_constant__ CUtensorMap mB_lo,
+                           const TcParams p) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* tfull = empty + STAGES;
+    uint64_t* tempty = tfull + 2;
+    uint64_t* drain = tempty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 128);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int total = p.m_tiles * p.n_tiles;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ------------------------------------------------ TMA producer
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t filled_phase[STAGES];
+            bool filled[STAGES];
+            for (int s = 0; s < STAGES; ++s) filled[s] = false, filled_phase[s] = 0;
+            bool ok = true;
+            const uint32_t tx = 2u * A_BYTES + 2u * (uint32_t)p.bn * ROW_BYTES;
+            for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+                const int nt = t % p.n_tiles, mt = t / p.n_tiles;
+                for (int kc = 0; kc < p.k_chunks; ++kc) {
+                    if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_PRODUCER)) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* st = smem + stage * STAGE_BYTES;
+                    mbar_expect_tx(&full[stage], tx);
+                    const int x = kc * p.elems_per_row;
+                    tma_load_2d(st, &mA_hi, &full[stage], x, mt * BM);
+                    tma_load_2d(st + A_BYTES, &mA_lo, &full[stage], x, mt * BM);
+                    tma_load_2d(st + 2 * A_BYTES, &mB_hi, &full[stage], x, nt * p.bn);
+                    tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mB_lo, &full[stage], x, nt * p.bn);
+                    filled[stage] = true;
+                    filled_phase[stage] = phase;
+                    if (++stage == STAGES) stage = 0, phase ^= 1;
+                }
+            }
+            if (!ok || *abort_flag) {
+                // Let the copies already issued land before the CTA exits.
+                for (int s = 0; s < STAGES; ++s)
+                    if (filled[s]) mbar_wait(&full[s], filled_phase[s], abort_flag, p.status, DEV_TIMEOUT_PRODUCER, true);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ------------------------------------------------ MMA issuer
+            const uint32_t idesc = instr_desc<KIND>(BM, p.bn);
+            int stage = 0, acc = 0;
+            uint32_t phase = 0, acc_phase = 0;
+            bool ok = true, issued = false;
+            for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+                if (!mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_MMA)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN_MAX);
+                for (int kc = 0; kc < p.k_chunks; ++kc) {
+                    if (!mbar_wait(&full[stage], phase, abort_flag, p.status, DEV_TIMEOUT_MMA)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t base = saddr(smem + stage * STAGE_BYTES);
+                    const uint64_t a_hi = smem_desc(base), a_lo = smem_desc(base + A_BYTES);
+                    const uint64_t b_hi = smem_desc(base + 2 * A_BYTES);
+                    const uint64_t b_lo = smem_desc(base + 2 * A_BYTES + B_BYTES);
+#pragma unroll
+                    for (int k = 0; k < ROW_BYTES / 32; ++k) {
+                        const uint64_t off = (uint64_t)((k * 32) >> 4);
+                        umma<KIND>(d_tmem, a_hi + off, b_hi + off, idesc, (kc | k) != 0);
+                        umma<KIND>(d_tmem, a_hi + off, b_lo + off, idesc, 1u);
+                        umma<KIND>(d_tmem, a_lo + off, b_hi + off, idesc, 1u);
+                    }
+                    umma_commit(&empty[stage]);
+                    issued = true;
+                    if (++stage == STAGES) stage = 0, phase ^= 1;
+                }
+                if (!ok) break;
+                umma_commit(&tfull[acc]);
+                if (++acc == 2) acc = 0, acc_phase ^= 1;
+            }
+            if ((!ok || *abort_flag) && issued) {
+                // Wait for every MMA this thread issued before TMEM is freed.
+                umma_commit(drain);
+                mbar_wait(drain, 0, abort_flag, p.status, DEV_TIMEOUT_MMA, true);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------------------------------------------- epilogue
+        const int q = warp & 3;  // TMEM lane quadrant this warp may access
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        const int chunks = (p.bn + 31) / 32;
+        for (int t = blockIdx.x; t < total; t += gridDim.x) {
+            const int nt = t % p.n_tiles, mt = t / p.n_tiles;
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait(&tfull[acc], acc_phase, abort_flag, p.status, DEV_TIMEOUT_EPILOGUE);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
+            tc_fence_after();
+            const int64_t row = (int64_t)mt * BM + q * 32 + lane;
+            const bool row_ok = row < p.R;
+            const int64_t row_off = row_ok ? (row % p.F) + p.F_pad * (row / p.F) : 0;
+            const int64_t col0 = (int64_t)nt * p.bn;
+            for (int ch = 0; ch < chunks; ++ch) {
+                uint32_t v[32];
+                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN_MAX + ch * 32), v);
+                if (row_ok) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int cj = ch * 32 + j;
+                        const int64_t col = col0 + cj;
+                        if (cj < p.bn && col < p.M) store_out(p, row_off + p.ldd * col, __uint_as_float(v[j]));
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&tempty[acc]);
+            if (++acc == 2) acc = 0, acc_phase ^= 1;
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
+using EncodeFn = PFN_cuTensorMapEncodeTiled_v12000;
+
+EncodeFn encode_fn() {
+    static EncodeFn fn = nullptr;
+    if (!fn) {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeFn>(ptr);
+    }
+    return fn;
+}
+
+int make_map(CUtensorMap* m, const void* base, int kind, int64_t K, int64_t rows, int64_t ld, int box_rows) {
+    EncodeFn enc = encode_fn();
+    if (!enc) return set_error(FCB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const int esz = kind == 1 ? 2 : 4;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (ld * esz) % 16 != 0)
+        return set_error(FCB_ERR_ARG, "split operand is not 16-byte aligned (padded leading dimension required)");
+    cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * esz)};
+    cuuint32_t box[2] = {(cuuint32_t)(ROW_BYTES / esz), (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, kind == 1 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                     const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(FCB_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return FCB_OK;
+}
+
+}  // namespace
+
+int pad_for(int kind, int64_t n) {
+    // TMA needs 16-byte row strides: 8 BF16 or 4 FP32 elements.
+    const int64_t q = kind == 1 ? 8 : 4;
+    return (int)(((n + q - 1) / q) * q);
+}
+
+int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A_lo, const void* B_hi,
+                    const void* B_lo, void* D_hi, void* D_lo, int out_kind, const ModeProduct& mp,
+                    cudaStream_t s) {
+    if (kind != 1 && kind != 2) return set_error(FCB_ERR_ARG, "mode_product_tc: bad operand kind");
+    if (mp.R <= 0 || mp.K <= 0 || mp.M <= 0) return FCB_OK;
+    TcParams p;
+    p.R = mp.R;
+    p.K = mp.K;
+    p.M = mp.M;
+    p.F = mp.F;
+    p.F_pad = mp.F_pad;
+    p.ldd = mp.ldd;
+    p.n_tiles = (int)((mp.M + BN_MAX - 1) / BN_MAX);
+    const int64_t per = (mp.M + p.n_tiles - 1) / p.n_tiles;
+    p.bn = (int)(((per + 15) / 16) * 16);
+    p.m_tiles = (int)((mp.R + BM - 1) / BM);
+    p.elems_per_row = ROW_BYTES / (kind == 1 ? 2 : 4);
+    p.k_chunks = (int)((mp.K + p.elems_per_row - 1) / p.elems_per_row);
+    p.out_kind = out_kind;
+    p.d_hi = D_hi;
+    p.d_lo = D_lo;
+    p.status = h->d_status;
+    CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
+    FCB_TRY(make_map(&ma_hi, A_hi, kind, mp.K, mp.R, mp.lda, BM));
+    FCB_TRY(make_map(&ma_lo, A_lo, kind, mp.K, mp.R, mp.lda, BM));
+    FCB_TRY(make_map(&mb_hi, B_hi, kind, mp.K, mp.M, mp.ldb, p.bn));
+    FCB_TRY(make_map(&mb_lo, B_lo, kind, mp.K, mp.M, mp.ldb, p.bn));
+    const int64_t tiles = (int64_t)p.m_tiles * p.n_tiles;
+    const int grid = (int)(tiles < h->sm_count ? tiles : h->sm_count);
+    if (kind == 1) {
+        static bool attr = false;
+        if (!attr) {
+            FCB_CUDA(cudaFuncSetAttribute(mode_product_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          SMEM_BYTES));
+            attr = true;
+        }
+        mode_product_tc_kernel<1><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(ma_hi, ma_lo, mb_hi, mb_lo, p);
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            FCB_CUDA(cudaFuncSetAttribute(mode_product_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          SMEM_BYTES));
+            attr = true;
+        }
+        mode_product_tc_kernel<2><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(ma_hi, ma_lo, mb_hi, mb_lo, p);
+    }
+    FCB_CUDA(cudaGetLastError());
+    return FCB_OK;
+}
+
+}  // namespace fcb

@@ -1,0 +1,20 @@
+"""fcb200 — B200-native third-order force constants and modal coupling constants.
+
+Host-side mirror of the ForceConstants.jl API for its dense IFC3 + mcc3 path,
+calling the C ABI of ``libfcb200.so`` (``include/fcb200.h``).
+"""
+from .crystals import FCC, Diamond, displaced
+from .ifc import (asr_satisfied, dynamical_matrix, get_modes, mass_weight_third_order_, second_order,
+                  second_order_, third_order, third_order_)
+from .mcc import mcc3, mcc3_, mcc3_tens_opt, mcc3_window, snapshot_lj
+from .types import (LJ, AnalyticalCalculator, AutoDiffCalculator, DenseForceConstants, PairPotential, Potential,
+                    StillingerWeberSilicon, SuperCellSystem, ThreeBodyPotential, energy_unit, length_unit, masses,
+                    n_atoms, positions)
+
+__all__ = [
+    "FCC", "Diamond", "displaced", "asr_satisfied", "dynamical_matrix", "get_modes", "mass_weight_third_order_",
+    "second_order", "second_order_", "third_order", "third_order_", "mcc3", "mcc3_", "mcc3_tens_opt",
+    "mcc3_window", "snapshot_lj", "LJ", "AnalyticalCalculator", "AutoDiffCalculator", "DenseForceConstants",
+    "PairPotential", "Potential", "StillingerWeberSilicon", "SuperCellSystem", "ThreeBodyPotential",
+    "energy_unit", "length_unit", "masses", "n_atoms", "positions",
+]

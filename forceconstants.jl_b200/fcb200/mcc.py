@@ -1,0 +1,92 @@
+"""Modal coupling constants mirroring ForceConstants.jl ``src/mcc.jl``.
+
+* ``mcc3(psi, phi)``               mcc.jl:29-51 — result stays on the device
+* ``mcc3(psi, phi, block_size)``   mcc.jl:89-120 — result is a host array
+* ``mcc3_(psi, phi)``              mcc.jl:60-80 (``mcc3!``; Ψ is left intact here)
+* ``mcc3_tens_opt(psi, phi)``      mcc.jl:11-20
+
+``precision`` selects the arithmetic of the three mode products: "fp32" (FFMA,
+the reference's Float32), "bf16x3" or "tf32x3" (split operands on the tensor
+cores, FP32 accumulation).  ``modes=(lo, hi)`` restricts every mode axis to
+φ[:, lo:hi] (0-based, half-open).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from .arrays import as_julia, device_index, is_torch, julia_empty, ptr, stream_ptr
+
+
+def _prep(psi, phi):
+    psi = as_julia(psi, np.float32)
+    phi = as_julia(phi, np.float32)
+    n = int(phi.shape[0])
+    if tuple(psi.shape) != (n, n, n) or tuple(phi.shape) != (n, n):
+        raise ValueError("Ψ must be n×n×n and φ n×n")
+    return psi, phi, n
+
+
+def mcc3(psi, phi, block_size: int | None = None, precision: str = "fp32", modes=None):
+    psi, phi, n = _prep(psi, phi)
+    prec = _lib.PRECISIONS[precision]
+    dev = device_index(psi) if is_torch(psi) else device_index(phi)
+    if block_size is not None and not (block_size > 0 and n % block_size == 0):
+        raise AssertionError("size(phi)[1] % block_size == 0")  # mcc.jl:91-92
+    h = _lib.handle(dev)
+    if block_size is not None:
+        out = np.empty((n, n, n), dtype=np.float32, order="F")
+        _lib.check(_lib.lib().fcb200_mcc3_blocked(h, ptr(psi), ptr(phi), n, int(block_size), prec, ptr(out),
+                                                  stream_ptr(psi)))
+        return out
+    lo, hi = (0, n) if modes is None else (int(modes[0]), int(modes[1]))
+    M = hi - lo
+    device = f"cuda:{dev}" if (is_torch(psi) and psi.is_cuda) else "cpu"
+    if device == "cpu" and is_torch(phi) and phi.is_cuda:
+        device = f"cuda:{dev}"
+    out = julia_empty((M, M, M), np.float32, device)
+    _lib.check(_lib.lib().fcb200_mcc3(h, ptr(psi), ptr(phi), n, lo, hi, lo, hi, lo, hi, prec, ptr(out),
+                                      stream_ptr(psi) or stream_ptr(phi)))
+    return out
+
+
+def mcc3_(psi, phi, precision: str = "fp32"):
+    """``mcc3!``: the reference overwrites Ψ as scratch; here Ψ is left intact
+    (the intermediates live in library scratch) and K3 is returned."""
+    return mcc3(psi, phi, precision=precision)
+
+
+def mcc3_tens_opt(psi, phi, precision: str = "fp32"):
+    return mcc3(psi, phi, precision=precision)
+
+
+def mcc3_window(psi, phi, n_range, m_range, l_range, precision: str = "fp32"):
+    """One block of mcc3_blocked! (mcc.jl:123-134): K3 over three mode windows."""
+    psi, phi, n = _prep(psi, phi)
+    prec = _lib.PRECISIONS[precision]
+    dev = device_index(psi) if is_torch(psi) else device_index(phi)
+    shape = (n_range[1] - n_range[0], m_range[1] - m_range[0], l_range[1] - l_range[0])
+    device = f"cuda:{dev}" if (is_torch(psi) and psi.is_cuda) else "cpu"
+    out = julia_empty(shape, np.float32, device)
+    _lib.check(_lib.lib().fcb200_mcc3(_lib.handle(dev), ptr(psi), ptr(phi), n, n_range[0], n_range[1],
+                                      m_range[0], m_range[1], l_range[0], l_range[1], prec, ptr(out),
+                                      stream_ptr(psi)))
+    return out
+
+
+def snapshot_lj(sys, pot, calc, phi, precision: str = "bf16x3", modes=None, psi_out=None, k3_out=None,
+                stream: int = 0):
+    """Fused third_order → mass_weight_third_order! → Float32 → mcc3 for one
+    LJ snapshot, without the host round trip.  Buffers may be host or device;
+    returns (psi_out, k3_out)."""
+    n = 3 * sys.n_atoms
+    lo, hi = (0, n) if modes is None else (int(modes[0]), int(modes[1]))
+    M = hi - lo
+    if k3_out is None:
+        k3_out = julia_empty((M, M, M), np.float32, "cuda" if is_torch(phi) and phi.is_cuda else "cpu")
+    dev = device_index(phi) if is_torch(phi) else 0
+    _lib.check(_lib.lib().fcb200_snapshot_lj(
+        _lib.handle(dev), ptr(sys.positions), sys.n_atoms, ptr(sys.box_sizes), float(pot.sigma), float(pot.eps),
+        float(calc.r_cut), float(calc.tol), ptr(sys.masses), ptr(phi), lo, hi, _lib.PRECISIONS[precision],
+        ptr(psi_out), ptr(k3_out), stream or stream_ptr(k3_out)))
+    return psi_out, k3_out

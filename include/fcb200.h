@@ -1,0 +1,178 @@
+/*
+ * fcb200 — B200-native third-order force constants and modal coupling constants.
+ *
+ * A C ABI over hand-written sm_100a kernels.  It is the drop-in target for the
+ * ForceConstants.jl hot path: dense third-order IFC assembly (LJ analytical and
+ * Stillinger-Weber), acoustic-sum-rule self terms, the tolerance cutoff, mass
+ * weighting and the `mcc3` modal contraction
+ *     K3[n,m,l] = Σ_ijk Ψ[i,j,k] φ[i,n] φ[j,m] φ[k,l].
+ *
+ * Conventions (all entry points):
+ *  - Every function returns an int status (FCB_OK = 0).  No exception or abort
+ *    crosses the ABI; fcb200_last_error() returns the message of the calling
+ *    thread's last failure.
+ *  - Sizes are int64_t.  Arrays are column-major (Julia layout).  Degree of
+ *    freedom index = 3*(atom) + component, 0-based here (Julia's 3(a-1)+α).
+ *    Ψ[ii,jj,kk] lives at ii + n*(jj + n*kk), n = 3*n_atoms.
+ *  - Positions are pos[3*a + x] (Julia's Vector{SVector{3}} flattened).
+ *  - Pointers may be host or device memory unless noted; the library detects
+ *    which (cudaPointerGetAttributes) and stages host buffers itself.
+ *  - `stream` is a cudaStream_t (NULL = the legacy default stream).  Calls with
+ *    only device buffers are asynchronous on that stream; calls that read or
+ *    write a host buffer synchronise the stream before returning.
+ *  - The caller owns every buffer it passes.  A handle owns the library's
+ *    scratch (pair tables, split operands, mode-product intermediates) and
+ *    caches it between calls.  A handle is not thread-safe; use one per thread.
+ */
+#ifndef FCB200_H
+#define FCB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define FCB_OK              0
+#define FCB_ERR_ARG         1  /* null pointer, bad size, inconsistent shape              */
+#define FCB_ERR_CUTOFF      2  /* r_cut not below the box (third_order_analytical.jl:7)   */
+#define FCB_ERR_OOM         3  /* device memory / admission refused                       */
+#define FCB_ERR_CUDA        4  /* CUDA runtime or driver error                            */
+#define FCB_ERR_TIMEOUT     5  /* a bounded device-side wait gave up (status word set)     */
+#define FCB_ERR_UNSUPPORTED 6  /* device is not sm_100 / precision not available          */
+#define FCB_ERR_BLOCK       7  /* size(phi,1) % block_size != 0 (mcc.jl:91-92)            */
+
+/* ---- mcc3 precision modes ------------------------------------------------ */
+#define FCB_MCC3_FP32       0  /* plain FP32 SIMT mode products (FFMA)                     */
+#define FCB_MCC3_BF16X3     1  /* split-BF16 on tcgen05: hi·hi + hi·lo + lo·hi, FP32 acc   */
+#define FCB_MCC3_TF32X3     2  /* split-TF32 on tcgen05: hi·hi + hi·lo + lo·hi, FP32 acc   */
+
+/* ---- flags for fcb200_third_order_* -------------------------------------- */
+#define FCB_PSI_MASS_WEIGHTED 1 /* write Ψ already divided by sqrt(m_i m_j m_k) into psi_out */
+
+typedef struct fcb200_context* fcb200_handle;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int fcb200_version(void);
+
+/* Copies the calling thread's last error message into buf (always terminated).
+ * Returns the status code of that error. */
+int fcb200_last_error(char* buf, size_t len);
+
+/* Creates a handle bound to CUDA device `device`.  Fails with
+ * FCB_ERR_UNSUPPORTED on devices other than compute capability 10.x. */
+int fcb200_create(fcb200_handle* out, int device);
+int fcb200_destroy(fcb200_handle h);
+
+/* Releases the cached scratch of a handle (kept otherwise until destroy). */
+int fcb200_trim(fcb200_handle h);
+
+/* Synchronises `stream` and reports a device-side error recorded by a
+ * bounded wait (FCB_ERR_TIMEOUT) since the last check. */
+int fcb200_synchronize(fcb200_handle h, void* stream);
+
+/*
+ * Dense third-order IFCs of a pair Lennard-Jones system with the analytical
+ * calculator.  Replaces
+ *   third_order(sys, pot::LJ, AnalyticalCalculator(tol, r_cut))   src/ifc.jl:20-35
+ *   third_order!(Ψ, sys, ::PairPotential, ::AnalyticalCalculator)
+ *                                        src/analytical/third_order_analytical.jl:4-69
+ *   ASR!(ifc3, N, D)                     src/asr.jl:19-40
+ *   apply_tols!(Ψ, tol)                  src/helper_funcs.jl:20-27
+ * and, fused into the same pass,
+ *   mass_weight_third_order!(Ψ, masses)  src/analytical/third_order_analytical.jl:185-214
+ *   CuArray{Float32}(Ψ_mw)               README.md:73-75
+ *
+ * pos       3*n_atoms doubles (Å), box 3 doubles (orthorhombic box lengths).
+ * sigma,eps LJ parameters (any consistent units; Ψ is in eps/length³).
+ * masses    n_atoms doubles, or NULL (required when psi32_mw_out is given or
+ *           flags has FCB_PSI_MASS_WEIGHTED).
+ * psi_out   n³ doubles or NULL: Ψ after ASR and tol (mass weighted if flagged).
+ * psi32_mw_out  n³ floats or NULL: FP32 copy of the mass-weighted Ψ.
+ * Returns FCB_ERR_CUTOFF when r_cut >= a box length (the reference asserts
+ * r_cut < L, third_order_analytical.jl:7).
+ */
+int fcb200_third_order_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                          double sigma, double eps, double r_cut, double tol,
+                          const double* masses, double* psi_out, float* psi32_mw_out,
+                          int flags, void* stream);
+
+/*
+ * In-place mass weighting of a dense third-order IFC tensor: every non-zero
+ * Ψ[ii,jj,kk] /= sqrt(m_i*m_j*m_k).  Replaces
+ *   mass_weight_third_order!(Ψ, masses)  src/analytical/third_order_analytical.jl:185-214
+ */
+int fcb200_mass_weight3(fcb200_handle h, double* psi, const double* masses, int64_t n_atoms,
+                        void* stream);
+
+/*
+ * Dense second-order IFCs (n×n) of an LJ system with the analytical calculator.
+ * Replaces second_order(sys, pot::LJ, AnalyticalCalculator)  src/ifc.jl:3-18,
+ * second_order!  src/analytical/second_order_analytical.jl:3-42, ASR!(ifc2)
+ * src/asr.jl:3-17.  With masses != NULL the result is the dynamical matrix
+ * (dynamical_matrix, src/dynmat.jl:5-33).
+ */
+int fcb200_second_order_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                           double sigma, double eps, double r_cut, double tol,
+                           const double* masses, double* ifc2_out, void* stream);
+
+/*
+ * Third-order modal coupling constants
+ *   K3[a,b,c] = Σ_ijk Ψ[i,j,k] φ[i,n_lo+a] φ[j,m_lo+b] φ[k,l_lo+c]
+ * for the mode windows [n_lo,n_hi) × [m_lo,m_hi) × [l_lo,l_hi), as three
+ * successive mode products.  Replaces
+ *   mcc3(Ψ::CuArray{Float32,3}, φ::CuArray{Float32,2})     src/mcc.jl:29-51
+ *   mcc3!(Ψ, φ) / mcc3_tens_opt(Ψ, φ)                       src/mcc.jl:11-20, 60-80
+ *   mcc3_blocked!(K3, Ψ, φ, ranges)  (one block)            src/mcc.jl:123-134
+ * psi    n³ floats (mass-weighted Ψ), phi n×n floats (columns = modes),
+ * k3_out (n_hi-n_lo)(m_hi-m_lo)(l_hi-l_lo) floats, column-major.
+ * precision is one of FCB_MCC3_*.
+ */
+int fcb200_mcc3(fcb200_handle h, const float* psi, const float* phi, int64_t n,
+                int64_t n_lo, int64_t n_hi, int64_t m_lo, int64_t m_hi, int64_t l_lo, int64_t l_hi,
+                int precision, float* k3_out, void* stream);
+
+/*
+ * Full K3 computed block-wise with a bounded device footprint.  Replaces
+ *   mcc3(Ψ, φ, block_size)   src/mcc.jl:89-120
+ * The result (n³ floats) is normally a host buffer, as in the reference; the
+ * (n/block_size) slabs of the last mode axis are copied back while the next
+ * slab computes.  Fails with FCB_ERR_BLOCK unless n % block_size == 0 and
+ * block_size > 0 (mcc.jl:91-92).
+ */
+int fcb200_mcc3_blocked(fcb200_handle h, const float* psi, const float* phi, int64_t n,
+                        int64_t block_size, int precision, float* k3_out, void* stream);
+
+/*
+ * One LJ snapshot end to end: dense FP64 IFC3 assembly (+ASR, tol), fused
+ * mass weighting into the operand format of the chosen precision, then mcc3
+ * over modes [mode_lo, mode_hi) on every axis.  The composition of
+ *   third_order (src/ifc.jl:20-35), mass_weight_third_order!
+ *   (third_order_analytical.jl:185-214), the Float32 cast (README.md:73-75)
+ *   and mcc3 (src/mcc.jl:29-51)
+ * without the host round trip.  psi_out (n³ doubles, unweighted) may be NULL;
+ * k3_out holds (mode_hi-mode_lo)³ floats.
+ */
+int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                       double sigma, double eps, double r_cut, double tol, const double* masses,
+                       const float* phi, int64_t mode_lo, int64_t mode_hi, int precision,
+                       double* psi_out, float* k3_out, void* stream);
+
+/*
+ * Device-side phase timing (no counterpart in the reference, which has no
+ * instrumentation).  With profiling enabled, fcb200_snapshot_lj records CUDA
+ * events on the caller's stream between its phases; fcb200_phase_times then
+ * returns (waiting for the last event) up to 6 durations in ms:
+ *   [0] pair tables + ASR self terms, [1] dense IFC3 write (+ fused mass-weighted
+ *   operand), [2] φ split, [3] mode product 1, [4] mode product 2,
+ *   [5] mode product 3.  A phase that did not run reports -1.
+ */
+int fcb200_set_profiling(fcb200_handle h, int enable);
+int fcb200_phase_times(fcb200_handle h, double* ms, int max_phases);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FCB200_H */

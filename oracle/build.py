@@ -1,0 +1,64 @@
+"""ORACLE build recipe — test infrastructure only.
+
+Compiles the CPU restatements under ``oracle/`` into ``oracle/liboracle.so``
+(gcc, OpenMP, no fused multiply-add so that evaluation order is exactly the
+order written in the C source).  When the ForceConstants.jl sources are present
+on this machine, also translates the reference's machine-generated
+Stillinger-Weber derivative kernels into C under ``oracle/_ref/`` and compiles
+them into ``oracle/_ref/libswref.so`` (see ``oracle/translate_sw_ref.py``).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_OUT = os.path.join(HERE, "_ref")
+SOURCES = ["lj_oracle.c", "sw_oracle.c"]
+LIB = os.path.join(HERE, "liboracle.so")
+CFLAGS = ["-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-std=c11"]
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_oracle(force: bool = False) -> str:
+    srcs = [os.path.join(HERE, s) for s in SOURCES if os.path.exists(os.path.join(HERE, s))]
+    if force or _stale(LIB, srcs):
+        cmd = ["gcc", *CFLAGS, *srcs, "-o", LIB, "-lm"]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+def build_reference_translation(reference_root: str | None = None, force: bool = False) -> str | None:
+    """Translate + compile the reference's generated SW derivative kernels.
+
+    Returns the path of ``oracle/_ref/libswref.so``, or None when the reference
+    sources are not on this machine and no previously built library exists.
+    """
+    from translate_sw_ref import translate_all  # noqa: E402  (sibling module)
+
+    reference_root = reference_root or os.environ.get("FCB200_REFERENCE_ROOT", "/root/reference")
+    lib = os.path.join(REF_OUT, "libswref.so")
+    gen_dir = os.path.join(reference_root, "src", "autodiff", "generated_derivatives")
+    if not os.path.isdir(gen_dir):
+        return lib if os.path.exists(lib) else None
+    os.makedirs(REF_OUT, exist_ok=True)
+    c_path = os.path.join(REF_OUT, "sw_generated.c")
+    if force or not os.path.exists(c_path) or not os.path.exists(lib):
+        translate_all(gen_dir, c_path)
+        cmd = ["gcc", "-O1", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", c_path,
+               "-o", lib, "-lm"]
+        subprocess.run(cmd, check=True)
+    return lib
+
+
+if __name__ == "__main__":
+    sys.path.insert(0, HERE)
+    print(build_oracle(force="--force" in sys.argv))
+    print(build_reference_translation(force="--force" in sys.argv))

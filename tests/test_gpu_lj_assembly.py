@@ -1,0 +1,136 @@
+"""LJ IFC2/IFC3 assembly on the GPU vs the CPU oracle (bit-exact) and the
+reference's golden values.
+
+Oracle: oracle/lj_oracle.c (restatement of third_order_analytical.jl:4-69,
+asr.jl:19-40, helper_funcs.jl:20-27, third_order_analytical.jl:185-214).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import AR, fcc_system
+
+pytestmark = pytest.mark.gpu
+
+CASES = [((2, 2, 2), 0.0, 0), ((2, 2, 2), 0.05, 11), ((3, 3, 3), 0.05, 12), ((3, 3, 2), 0.08, 13)]
+
+
+def _pot_calc(fcb, tol=1e-12):
+    return fcb.LJ(AR["sigma"], AR["eps"], AR["r_cut"]), fcb.AnalyticalCalculator(tol, AR["r_cut"])
+
+
+def _cpu(t):
+    return t.cpu().numpy() if hasattr(t, "cpu") else t
+
+
+@pytest.mark.parametrize("cells,std,seed", CASES)
+def test_third_order_bit_exact(fcb, oracle, cuda_device, cells, std, seed):
+    s = fcc_system(cells, std, seed)
+    pot, calc = _pot_calc(fcb)
+    ref = oracle.third_order_lj(s.positions, s.box_sizes, pot.sigma, pot.eps, pot.r_cut, calc.tol)
+    got = fcb.third_order(s, pot, calc, device="cuda")
+    g = _cpu(got.values)
+    assert g.shape == ref.shape
+    assert np.array_equal(g, ref), f"max |Δ| = {np.max(np.abs(g - ref))}"
+
+
+@pytest.mark.parametrize("cells,std,seed", CASES[1:3])
+def test_mass_weighted_and_fp32_copy(fcb, oracle, cuda_device, cells, std, seed):
+    import torch
+    s = fcc_system(cells, std, seed)
+    s.masses[:] = np.linspace(35.0, 45.0, s.n_atoms)
+    pot, calc = _pot_calc(fcb)
+    n = 3 * s.n_atoms
+    ref = oracle.third_order_lj(s.positions, s.box_sizes, pot.sigma, pot.eps, pot.r_cut, calc.tol)
+    ref_mw = oracle.mass_weight_third_order(ref.copy(order="F"), s.masses)
+    from fcb200.arrays import julia_empty
+    psi = julia_empty((n, n, n), np.float64, "cuda")
+    psi32 = julia_empty((n, n, n), np.float32, "cuda")
+    fcb.third_order_(psi, s, pot, calc, mass_weighted=True, psi32_mw=psi32)
+    torch.cuda.synchronize()
+    assert np.array_equal(_cpu(psi), ref_mw)
+    f32 = np.empty(ref_mw.size, dtype=np.float32)
+    oracle.lib().oracle_cast_f32(oracle._pd(ref_mw.reshape(-1, order="F")),
+                                 f32.ctypes.data_as(oracle._PF), ref_mw.size)
+    assert np.array_equal(_cpu(psi32), f32.reshape(ref_mw.shape, order="F"))
+
+
+def test_mass_weight_in_place_matches_oracle(fcb, oracle, cuda_device):
+    s = fcc_system((2, 2, 2), 0.05, 5)
+    pot, calc = _pot_calc(fcb)
+    m = np.linspace(20.0, 60.0, s.n_atoms)
+    ifc3 = fcb.third_order(s, pot, calc, device="cuda")
+    ref = oracle.mass_weight_third_order(_cpu(ifc3.values).copy(order="F"), m)
+    fcb.mass_weight_third_order_(ifc3, m)
+    assert np.array_equal(_cpu(ifc3.values), ref)
+    # host-buffer form of the same entry point
+    host = fcb.third_order(s, pot, calc)
+    fcb.mass_weight_third_order_(host, m)
+    assert np.array_equal(host.values, ref)
+
+
+def test_host_output_equals_device_output(fcb, cuda_device):
+    s = fcc_system((2, 2, 2), 0.05, 9)
+    pot, calc = _pot_calc(fcb)
+    a = fcb.third_order(s, pot, calc)              # host array, like the reference
+    b = fcb.third_order(s, pot, calc, device="cuda")
+    assert isinstance(a.values, np.ndarray) and a.values.flags.f_contiguous
+    assert np.array_equal(a.values, _cpu(b.values))
+
+
+def test_golden_values_on_device(fcb, cuda_device):
+    with open(os.path.join(os.path.dirname(__file__), "golden", "lj_values.json")) as f:
+        golden = json.load(f)
+    s = fcc_system((4, 4, 4))
+    pot, calc = _pot_calc(fcb, tol=1e-8)
+    ifc2 = fcb.second_order(s, pot, calc)
+    ifc3 = fcb.third_order(s, pot, calc, device="cuda")
+    rtol = golden["rtol"]
+    for g in golden["ifc2"]:
+        i, j = (x - 1 for x in g["index_1based"])
+        assert abs(ifc2[i, j] - g["value"]) <= rtol * abs(g["value"])
+    for g in golden["ifc3"]:
+        i, j, k = (x - 1 for x in g["index_1based"])
+        v = float(ifc3.values[i, j, k])
+        if g["value"] == 0.0:
+            assert v == 0.0
+        else:
+            assert abs(v - g["value"]) <= rtol * abs(g["value"]), (g, v)
+    assert fcb.asr_satisfied(ifc2.values, 256, 3, 1e-8)
+    assert np.array_equal(ifc2.values, ifc2.values.T)
+
+
+@pytest.mark.parametrize("cells,std,seed", [((2, 2, 2), 0.05, 3), ((3, 3, 3), 0.0, 0)])
+def test_second_order_and_dynmat_bit_exact(fcb, oracle, cuda_device, cells, std, seed):
+    s = fcc_system(cells, std, seed)
+    pot, calc = _pot_calc(fcb)
+    ref = oracle.second_order_lj(s.positions, s.box_sizes, pot.sigma, pot.eps, pot.r_cut, calc.tol)
+    got = fcb.second_order(s, pot, calc)
+    assert np.array_equal(got.values, ref)
+    dyn = fcb.dynamical_matrix(s, pot, calc)
+    assert np.allclose(dyn.values, oracle.dynamical_matrix(ref, s.masses), rtol=1e-15, atol=0)
+
+
+def test_cutoff_error_is_reported(fcb, cuda_device):
+    s = fcc_system((1, 1, 1))
+    pot, calc = _pot_calc(fcb)
+    from fcb200 import _lib
+    import ctypes
+    n = 12
+    buf = np.zeros(n ** 3)
+    st = _lib.lib().fcb200_third_order_lj(_lib.handle(0), s.positions.ctypes.data, s.n_atoms,
+                                          s.box_sizes.ctypes.data, pot.sigma, pot.eps, pot.r_cut, 1e-12,
+                                          None, buf.ctypes.data, None, 0, None)
+    assert st == _lib.FCB_ERR_CUTOFF
+    with pytest.raises(AssertionError, match="Cutoff"):
+        fcb.third_order(s, pot, calc)
+
+
+def test_deterministic_repeat(fcb, cuda_device):
+    s = fcc_system((3, 3, 3), 0.05, 21)
+    pot, calc = _pot_calc(fcb)
+    a = _cpu(fcb.third_order(s, pot, calc, device="cuda").values)
+    b = _cpu(fcb.third_order(s, pot, calc, device="cuda").values)
+    assert np.array_equal(a, b)

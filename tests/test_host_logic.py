@@ -1,0 +1,69 @@
+"""Host-side logic of the Python mirror (no GPU needed)."""
+import numpy as np
+import pytest
+
+from conftest import AR, fcc_system
+
+
+def test_fcc_ordering_matches_reference_golden_layout(fcb):
+    s = fcb.FCC(AR["a"], "Ar", (4, 4, 4))
+    assert s.n_atoms == 256
+    assert np.allclose(s.positions[0], 0.0)
+    # Atom 2 sits at (a/2, a/2, 0): the layout the reference's golden values imply.
+    assert np.allclose(s.positions[1], [AR["a"] / 2, AR["a"] / 2, 0.0])
+    assert np.allclose(s.box_sizes, 4 * AR["a"])
+    assert np.allclose(s.masses, 39.95)
+
+
+def test_diamond_builder(fcb):
+    s = fcb.Diamond(5.43, "Si", (3, 3, 3))
+    assert s.n_atoms == 216
+    d = s.positions[:, None, :] - s.positions[None, :, :]
+    d -= np.round(d / s.box_sizes) * s.box_sizes
+    r = np.sqrt((d ** 2).sum(-1))
+    nn = np.sort(r, axis=1)[:, 1:5]
+    assert np.allclose(nn, 5.43 * np.sqrt(3) / 4)
+
+
+def test_displacement_is_seeded(fcb):
+    a = fcb.displaced(fcc_system((2, 2, 2)), 0.05, seed=7)
+    b = fcb.displaced(fcc_system((2, 2, 2)), 0.05, seed=7)
+    assert np.array_equal(a.positions, b.positions)
+
+
+def test_cutoff_assertion_before_any_device_work(fcb):
+    s = fcc_system((1, 1, 1))
+    calc = fcb.AnalyticalCalculator(1e-12, AR["r_cut"])
+    pot = fcb.LJ(AR["sigma"], AR["eps"], AR["r_cut"])
+    psi = np.zeros((12, 12, 12), order="F")
+    with pytest.raises(AssertionError, match="Cutoff"):
+        fcb.third_order_(psi, s, pot, calc)
+
+
+def test_julia_layout_helpers(fcb):
+    import torch
+    from fcb200.arrays import as_julia, julia_empty
+    x = torch.arange(24, dtype=torch.float32).reshape(2, 3, 4)
+    j = as_julia(x, np.float32)
+    assert j.stride() == (1, 2, 6)
+    assert torch.equal(j, x)
+    e = julia_empty((3, 4, 5), np.float64, "cpu")
+    assert e.flags.f_contiguous
+    a = np.arange(24.0).reshape(2, 3, 4)
+    assert as_julia(a, np.float64).flags.f_contiguous
+
+
+def test_block_size_assertion(fcb):
+    psi = np.zeros((6, 6, 6), dtype=np.float32, order="F")
+    phi = np.eye(6, dtype=np.float32)
+    with pytest.raises(AssertionError):
+        fcb.mcc3(psi, phi, 4)
+
+
+def test_asr_checker_quirk(fcb):
+    # asr.jl:50 tests `s > tol` without abs: a negative sum passes.
+    ifc2 = np.zeros((3, 3))
+    ifc2[0, 0] = -1.0
+    assert fcb.asr_satisfied(ifc2, 1, 3, 1e-8)
+    ifc2[0, 0] = 1.0
+    assert not fcb.asr_satisfied(ifc2, 1, 3, 1e-8)
