@@ -41,6 +41,8 @@ def build_reference_translation(reference_root: str | None = None, force: bool =
     Returns the path of ``oracle/_ref/libswref.so``, or None when the reference
     sources are not on this machine and no previously built library exists.
     """
+    if HERE not in sys.path:
+        sys.path.append(HERE)
     from translate_sw_ref import translate_all  # noqa: E402  (sibling module)
 
     reference_root = reference_root or os.environ.get("FCB200_REFERENCE_ROOT", "/root/reference")
