@@ -112,6 +112,10 @@ int lj_pair_tables(fcb200_context* h, const double* d_pos, int64_t N, const doub
 int ifc3_dense_write(fcb200_context* h, int64_t N, double tol, const double* d_masses,
                      const AssemblyOut& out, cudaStream_t s);
 int mass_weight3_launch(double* d_psi, const double* d_masses, int64_t N, cudaStream_t s);
+int lj_pair_tables_raw(double* T, uint8_t* flag, double* S, const double* d_pos, int64_t N, const double* d_box,
+                       double sigma, double eps, double r_cut, cudaStream_t s);
+int ifc3_dense_write_raw(const double* T, const uint8_t* flag, const double* S, int sm_count, int64_t N, double tol,
+                         const double* d_masses, const AssemblyOut& out, cudaStream_t s);
 int lj_second_order_launch(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box,
                            double sigma, double eps, double r_cut, double tol,
                            const double* d_masses, double* d_ifc2, cudaStream_t s);

@@ -416,4 +416,48 @@ int lj_second_order_launch(fcb200_context* h, const double* d_pos, int64_t N, co
     return FCB_OK;
 }
 
+
+// Launchers over caller-provided scratch (T: N*N*27 doubles, flag: N*N bytes,
+// S: N*27 doubles).  Same kernels as above; used by the entry point whose
+// scratch is a fixed device array instead of handle-owned allocations.
+int lj_pair_tables_raw(double* T, uint8_t* flag, double* S, const double* d_pos, int64_t N, const double* d_box,
+                       double sigma, double eps, double r_cut, cudaStream_t s) {
+    const int64_t pairs = N * N;
+    const double rc2 = r_cut * r_cut;
+    lj_pair_kernel<<<(unsigned)((pairs + 127) / 128), 128, 0, s>>>(d_pos, d_box, N, sigma, eps, rc2, T, flag);
+    FCB_CUDA(cudaGetLastError());
+    lj_self_kernel<<<(unsigned)((N * 27 + 127) / 128), 128, 0, s>>>(N, T, flag, S);
+    FCB_CUDA(cudaGetLastError());
+    return FCB_OK;
+}
+
+int ifc3_dense_write_raw(const double* T, const uint8_t* flag, const double* S, int sm_count, int64_t N, double tol,
+                         const double* d_masses, const AssemblyOut& out, cudaStream_t s) {
+    DenseArgs g;
+    g.N = N;
+    g.n = 3 * N;
+    g.n_pad = out.n_pad ? out.n_pad : g.n;
+    g.tol = tol;
+    g.T = T;
+    g.flag = flag;
+    g.S = S;
+    g.masses = d_masses;
+    g.psi64 = out.psi64;
+    g.psi64_weighted = out.psi64_weighted;
+    g.psi32 = out.psi32;
+    g.split_hi = out.split_hi;
+    g.split_lo = out.split_lo;
+    g.split_kind = out.split_kind;
+    const int64_t cols = g.n * g.n;
+    int64_t blocks = (cols + 7) / 8;
+    const int64_t cap = (int64_t)sm_count * 8;
+    if (blocks > cap) blocks = cap;
+    if (g.n % 2 == 0 && g.n_pad % 2 == 0)
+        ifc3_dense_kernel<true><<<(unsigned)blocks, 256, 0, s>>>(g);
+    else
+        ifc3_dense_kernel<false><<<(unsigned)blocks, 256, 0, s>>>(g);
+    FCB_CUDA(cudaGetLastError());
+    return FCB_OK;
+}
+
 }  // namespace fcb

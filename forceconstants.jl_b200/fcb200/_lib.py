@@ -48,6 +48,7 @@ SIGNATURES = {
     "fcb200_snapshot_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _D, _P, _P, _I64, _I64, _I, _P, _P, _P]),
     "fcb200_set_profiling": (_I, [_P, _I]),
     "fcb200_phase_times": (_I, [_P, ctypes.POINTER(_D), _I]),
+    "fcb200_third_order_lj_noalloc": (_I, [_P, _I64, _P, _D, _D, _D, _D, _P, _P, _P, _I, _P]),
 }
 
 _lib = None

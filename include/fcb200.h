@@ -172,6 +172,32 @@ int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t n_atoms, cons
 int fcb200_set_profiling(fcb200_handle h, int enable);
 int fcb200_phase_times(fcb200_handle h, double* ms, int max_phases);
 
+/*
+ * LJ IFC3 assembly that allocates no device memory (no counterpart in the
+ * reference: it exists for callers that cannot let a library allocate).
+ * A Julia host keeps device memory in CUDA.jl's pool, whose accounting never
+ * sees allocations made inside a foreign library; programs that size all
+ * device memory at start-up have the same rule; and cudaFree synchronises the
+ * whole device, stalling callers that keep several streams busy.
+ *
+ * Same results as fcb200_third_order_lj (bit for bit), with these differences:
+ *  - no handle; pos, masses, psi_out and psi32_mw_out must be device memory,
+ *    box is a host array of 3 doubles;
+ *  - n_atoms <= FCB_NOALLOC_MAX_ATOMS, otherwise FCB_ERR_ARG before any work;
+ *  - its scratch is one fixed device array (about 14.3 MB) that every GPU
+ *    loading the library keeps until the process exits.  All calls share it
+ *    and it keeps the last call's contents (nothing in it needs to start at
+ *    zero); calls that overlap on the GPU race on it and must be serialised;
+ *  - the first call on a device looks up the array's address with that device
+ *    current; make that first call before any stream capture begins.
+ * Asynchronous on `stream`.
+ */
+#define FCB_NOALLOC_MAX_ATOMS 256
+int fcb200_third_order_lj_noalloc(const double* pos, int64_t n_atoms, const double* box,
+                                  double sigma, double eps, double r_cut, double tol,
+                                  const double* masses, double* psi_out, float* psi32_mw_out,
+                                  int flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
