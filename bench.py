@@ -239,7 +239,13 @@ def main():
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32x3", "fp32"])
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--cells", default=None, help="FCC cells 'x,y,z' (profiling cases; default 4,4,4)")
+    ap.add_argument("--minimal", action="store_true",
+                    help="warm-up + timed steps only (for profiler captures of small cases)")
     args = ap.parse_args()
+    if args.cells:
+        global CELLS
+        CELLS = tuple(int(c) for c in args.cells.split(","))
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -306,6 +312,16 @@ def main():
         ms = float(t.item())
     ms_per_step = ms / args.steps
     value = (ms / 1e3) / (args.steps * world)
+    if args.minimal:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                              "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False,
+                              "config": {"cells": list(CELLS), "n": n, "precision": args.precision},
+                              "clocks": clk, "minimal": True}), flush=True)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
 
     # ---- per-phase device times (profiled pass, same stream, outside the timed region)
     _lib.check(L.fcb200_set_profiling(h, 1))

@@ -279,6 +279,86 @@ __global__ void __launch_bounds__(256) ifc3_dense_kernel(DenseArgs g) {
     }
 }
 
+// Split pair (hi, lo) of two consecutive mass-weighted values.  The BF16 hi
+// part is rounded through FP32 (cvt.rn.f32.f64 then cvt.rn.bf16x2.f32); the lo
+// part captures the exact remainder to BF16 precision either way.
+__device__ __forceinline__ void split_pair(const DenseArgs& g, int64_t off, double w0, double w1) {
+    if (g.split_kind == 1) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn((float)w0, (float)w1);
+        const float h0 = __low2float(h), h1 = __high2float(h);
+        const __nv_bfloat162 l = __floats2bfloat162_rn((float)(w0 - (double)h0), (float)(w1 - (double)h1));
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(g.split_hi) + off) = h;
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(g.split_lo) + off) = l;
+    } else if (g.split_kind == 2) {
+        uint32_t b0, b1;
+        const float f0 = (float)w0, f1 = (float)w1;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b0) : "f"(f0));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b1) : "f"(f1));
+        const float h0 = __uint_as_float(b0), h1 = __uint_as_float(b1);
+        *reinterpret_cast<float2*>(static_cast<float*>(g.split_hi) + off) = make_float2(h0, h1);
+        *reinterpret_cast<float2*>(static_cast<float*>(g.split_lo) + off) =
+            make_float2((float)(w0 - (double)h0), (float)(w1 - (double)h1));
+    }
+}
+
+__device__ __forceinline__ void split_zero(const DenseArgs& g, int64_t off) {
+    if (g.split_kind == 1) {
+        *reinterpret_cast<uint32_t*>(static_cast<__nv_bfloat16*>(g.split_hi) + off) = 0u;
+        *reinterpret_cast<uint32_t*>(static_cast<__nv_bfloat16*>(g.split_lo) + off) = 0u;
+    } else if (g.split_kind == 2) {
+        *reinterpret_cast<float2*>(static_cast<float*>(g.split_hi) + off) = make_float2(0.f, 0.f);
+        *reinterpret_cast<float2*>(static_cast<float*>(g.split_lo) + off) = make_float2(0.f, 0.f);
+    }
+}
+
+// The dense writer for even n (every column starts on a 16-byte boundary).
+// Lane l writes elements (2l, 2l+1) of each 64-element group, so every warp
+// store instruction covers one contiguous segment (512 B of FP64, 128 B per
+// BF16 plane).  The column class is decided once per column; element values
+// are evaluated only for pairs that touch the rows of the column's atoms
+// (pair columns) or in self columns (J == K); everything else stores
+// constant zeros.
+__global__ void __launch_bounds__(256) ifc3_dense_kernel2(DenseArgs g) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int n = (int)g.n;
+    const int64_t N = g.N;
+    const int64_t ncols = (int64_t)n * n;
+    for (int64_t col = warp; col < ncols; col += nwarps) {
+        const int kk = (int)(col / n), jj = (int)(col - (int64_t)kk * n);
+        const int J = jj / 3, K = kk / 3;
+        const int b = jj - 3 * J, c = kk - 3 * K;
+        const bool self_col = (J == K);
+        const bool live = self_col || g.flag[(int64_t)J * N + K];
+        const int j0 = 3 * J, k0 = 3 * K;
+        double* p64 = g.psi64 ? g.psi64 + col * n : nullptr;
+        float* p32 = g.psi32 ? g.psi32 + col * n : nullptr;
+        const int64_t soff = col * g.n_pad;
+        for (int e = 2 * lane; e < n; e += 64) {
+            const bool touch = live && (self_col || (e + 2 > j0 && e < j0 + 3) || (e + 2 > k0 && e < k0 + 3));
+            if (!touch) {
+                if (p64) __stcs(reinterpret_cast<double2*>(p64 + e), make_double2(0.0, 0.0));
+                if (p32) __stcs(reinterpret_cast<float2*>(p32 + e), make_float2(0.f, 0.f));
+                split_zero(g, soff + e);
+                continue;
+            }
+            const double mJ = g.masses ? g.masses[J] : 0.0, mK = g.masses ? g.masses[K] : 0.0;
+            double r0 = 0.0, r1 = 0.0, w0 = 0.0, w1 = 0.0;
+            const int I0 = e / 3, I1 = (e + 1) / 3;
+            const int a0 = e - 3 * I0, a1 = e + 1 - 3 * I1;
+            if (self_col || I0 == J || I0 == K) finish(g, element_value(g, I0, a0, J, b, K, c), mJ, mK, I0, &r0, &w0);
+            if (self_col || I1 == J || I1 == K) finish(g, element_value(g, I1, a1, J, b, K, c), mJ, mK, I1, &r1, &w1);
+            if (p64) {
+                const double2 o = g.psi64_weighted ? make_double2(w0, w1) : make_double2(r0, r1);
+                __stcs(reinterpret_cast<double2*>(p64 + e), o);
+            }
+            if (p32) __stcs(reinterpret_cast<float2*>(p32 + e), make_float2((float)w0, (float)w1));
+            if (g.split_kind) split_pair(g, soff + e, w0, w1);
+        }
+    }
+}
+
 // In-place mass weighting (third_order_analytical.jl:185-214).
 template <bool VEC2>
 __global__ void __launch_bounds__(256) mass_weight3_kernel(double* __restrict__ psi,
@@ -383,7 +463,7 @@ int ifc3_dense_write(fcb200_context* h, int64_t N, double tol, const double* d_m
     const int64_t cap = (int64_t)h->sm_count * 8;
     if (blocks > cap) blocks = cap;
     if (g.n % 2 == 0 && g.n_pad % 2 == 0)
-        ifc3_dense_kernel<true><<<(unsigned)blocks, 256, 0, s>>>(g);
+        ifc3_dense_kernel2<<<(unsigned)blocks, 256, 0, s>>>(g);
     else
         ifc3_dense_kernel<false><<<(unsigned)blocks, 256, 0, s>>>(g);
     FCB_CUDA(cudaGetLastError());
@@ -453,7 +533,7 @@ int ifc3_dense_write_raw(const double* T, const uint8_t* flag, const double* S, 
     const int64_t cap = (int64_t)sm_count * 8;
     if (blocks > cap) blocks = cap;
     if (g.n % 2 == 0 && g.n_pad % 2 == 0)
-        ifc3_dense_kernel<true><<<(unsigned)blocks, 256, 0, s>>>(g);
+        ifc3_dense_kernel2<<<(unsigned)blocks, 256, 0, s>>>(g);
     else
         ifc3_dense_kernel<false><<<(unsigned)blocks, 256, 0, s>>>(g);
     FCB_CUDA(cudaGetLastError());

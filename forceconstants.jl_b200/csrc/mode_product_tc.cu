@@ -84,9 +84,8 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
 // Bounded wait.  Returns false (after flagging the CTA and the device status
 // word) when the phase does not complete within TIMEOUT_NS, or when another
 // role of this CTA has already given up (unless `ignore_abort`).
-__device__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag, int* status, int code,
-                          bool ignore_abort = false) {
-    if (mbar_try(b, parity)) return true;
+__device__ __noinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, volatile int* abort_flag, int* status,
+                                            int code, bool ignore_abort) {
     const uint64_t t0 = gtimer();
     while (true) {
         if (mbar_try(b, parity)) return true;
@@ -97,6 +96,12 @@ __device__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag
             return false;
         }
     }
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag, int* status,
+                                          int code, bool ignore_abort = false) {
+    if (mbar_try(b, parity)) return true;
+    return mbar_wait_slow(b, parity, abort_flag, status, code, ignore_abort);
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
@@ -172,7 +177,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ void store_out(const TcParams& p, int64_t off, float v) {
+__device__ __forceinline__ float tf32_round(float v) {
+    uint32_t hb;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(v));
+    return __uint_as_float(hb);
+}
+
+__device__ __forceinline__ void store_one(const TcParams& p, int64_t off, float v) {
     if (p.out_kind == 0) {
         static_cast<float*>(p.d_hi)[off] = v;
     } else if (p.out_kind == 1) {
@@ -180,11 +191,46 @@ __device__ __forceinline__ void store_out(const TcParams& p, int64_t off, float 
         static_cast<__nv_bfloat16*>(p.d_hi)[off] = h;
         static_cast<__nv_bfloat16*>(p.d_lo)[off] = __float2bfloat16_rn(v - __bfloat162float(h));
     } else {
-        uint32_t hb;
-        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(v));
-        const float h = __uint_as_float(hb);
+        const float h = tf32_round(v);
         static_cast<float*>(p.d_hi)[off] = h;
         static_cast<float*>(p.d_lo)[off] = v - h;
+    }
+}
+
+// A full chunk: this thread's row, 32 consecutive modes; element j goes to
+// off + j*ldd.  Lanes of the warp hold consecutive rows, so each store
+// instruction writes one contiguous segment per output plane.
+template <int OUT>
+__device__ __forceinline__ void store_chunk(const TcParams& p, int64_t off, const uint32_t (&v)[32]) {
+    const int64_t ldd = p.ldd;
+    if constexpr (OUT == 0) {
+        float* d = static_cast<float*>(p.d_hi) + off;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) d[j * ldd] = __uint_as_float(v[j]);
+    } else if constexpr (OUT == 1) {
+        __nv_bfloat16* dh = static_cast<__nv_bfloat16*>(p.d_hi) + off;
+        __nv_bfloat16* dl = static_cast<__nv_bfloat16*>(p.d_lo) + off;
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+            const float a = __uint_as_float(v[j]), b = __uint_as_float(v[j + 1]);
+            const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+            const uint32_t hu = *reinterpret_cast<const uint32_t*>(&h);
+            const __nv_bfloat162 l =
+                __floats2bfloat162_rn(a - __uint_as_float(hu << 16), b - __uint_as_float(hu & 0xFFFF0000u));
+            dh[j * ldd] = h.x;
+            dh[(j + 1) * ldd] = h.y;
+            dl[j * ldd] = l.x;
+            dl[(j + 1) * ldd] = l.y;
+        }
+    } else {
+        float* dh = static_cast<float*>(p.d_hi) + off;
+        float* dl = static_cast<float*>(p.d_lo) + off;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const float x = __uint_as_float(v[j]), h = tf32_round(x);
+            dh[j * ldd] = h;
+            dl[j * ldd] = x - h;
+        }
     }
 }
 
@@ -235,9 +281,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             // ------------------------------------------------ TMA producer
             int stage = 0;
             uint32_t phase = 0;
-            uint32_t filled_phase[STAGES];
-            bool filled[STAGES];
-            for (int s = 0; s < STAGES; ++s) filled[s] = false, filled_phase[s] = 0;
+            uint32_t filled = 0, filled_phase = 0;  // per-stage bit masks
             bool ok = true;
             const uint32_t tx = 2u * A_BYTES + 2u * (uint32_t)p.bn * ROW_BYTES;
             for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
@@ -254,15 +298,17 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     tma_load_2d(st + A_BYTES, &mA_lo, &full[stage], x, mt * BM);
                     tma_load_2d(st + 2 * A_BYTES, &mB_hi, &full[stage], x, nt * p.bn);
                     tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mB_lo, &full[stage], x, nt * p.bn);
-                    filled[stage] = true;
-                    filled_phase[stage] = phase;
+                    filled |= 1u << stage;
+                    filled_phase = (filled_phase & ~(1u << stage)) | (phase << stage);
                     if (++stage == STAGES) stage = 0, phase ^= 1;
                 }
             }
             if (!ok || *abort_flag) {
                 // Let the copies already issued land before the CTA exits.
                 for (int s = 0; s < STAGES; ++s)
-                    if (filled[s]) mbar_wait(&full[s], filled_phase[s], abort_flag, p.status, DEV_TIMEOUT_PRODUCER, true);
+                    if (filled & (1u << s))
+                        mbar_wait(&full[s], (filled_phase >> s) & 1u, abort_flag, p.status, DEV_TIMEOUT_PRODUCER,
+                                  true);
             }
         }
         __syncwarp();
@@ -332,13 +378,20 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             for (int ch = 0; ch < chunks; ++ch) {
                 uint32_t v[32];
                 tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN_MAX + ch * 32), v);
-                if (row_ok) {
+                if (!row_ok) continue;
+                const int64_t c0 = col0 + ch * 32;
+                const int64_t off = row_off + p.ldd * c0;
+                if (ch * 32 + 32 <= p.bn && c0 + 32 <= p.M) {
+                    if (p.out_kind == 1)
+                        store_chunk<1>(p, off, v);
+                    else if (p.out_kind == 0)
+                        store_chunk<0>(p, off, v);
+                    else
+                        store_chunk<2>(p, off, v);
+                } else {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int cj = ch * 32 + j;
-                        const int64_t col = col0 + cj;
-                        if (cj < p.bn && col < p.M) store_out(p, row_off + p.ldd * col, __uint_as_float(v[j]));
-                    }
+                    for (int j = 0; j < 32; ++j)
+                        if (ch * 32 + j < p.bn && c0 + j < p.M) store_one(p, off + p.ldd * j, __uint_as_float(v[j]));
                 }
             }
             tc_fence_before();
