@@ -38,6 +38,10 @@ UNIT = "s/snapshot"
 CELLS, A_LAT, STD, SEED = (4, 4, 4), 5.2468, 0.05, 1234
 SIGMA, EPS, R_CUT, TOL, MASS = 3.4, 0.24037, 8.5, 1e-12, 39.95
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+# DRAM bytes (read + write) per launch at n = 768 from one ncu capture of this
+# command (dram__bytes_read.sum + dram__bytes_write.sum, 1 pass):
+#   mode product (bf16x3): 1.816e9 + 1.767e9; dense IFC3 writer: 0.021e9 + 5.376e9
+NCU_TRAFFIC = {"mode_product_tc_bf16x3": 3.583e9, "ifc3_dense": 5.397e9}
 
 
 def load_peaks():
@@ -348,7 +352,9 @@ def main():
         pk = peaks["bf16_tflops_sustained"] if args.precision == "bf16x3" else None
         ach = flops_launch / (mp_ms * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": round(ach, 2), "peak": pk, "unit": "TFLOP/s",
-                "frac": round(ach / pk, 4) if pk else None, "traffic": None,
+                "frac": round(ach / pk, 4) if pk else None,
+                "traffic": NCU_TRAFFIC["mode_product_tc_bf16x3"] if (args.precision == "bf16x3" and n == 768) else None,
+                "traffic_unit": "bytes/launch (ncu, DRAM read+write)",
                 "kernel": f"mode_product_tc_kernel ({args.precision}), 3 launches/step",
                 "flops_per_launch": flops_launch, "avg_launch_ms": round(mp_ms, 4),
                 "peak_source": f"{peak_src} bf16_tflops_sustained (tensor flops executed = 3x useful for the split)"}
@@ -356,7 +362,7 @@ def main():
     asm_ms = float(phases[1])
     roof_asm = {"bound": "hbm", "achieved": round(asm_bytes / (asm_ms * 1e-3) / 1e9, 1), "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": round(asm_bytes / (asm_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4),
-                "traffic": None, "kernel": "ifc3_dense_kernel", "bytes_per_launch": asm_bytes,
+                "traffic": NCU_TRAFFIC["ifc3_dense"] if (args.precision == "bf16x3" and n == 768) else None, "kernel": "ifc3_dense_kernel", "bytes_per_launch": asm_bytes,
                 "avg_launch_ms": round(asm_ms, 4)}
 
     # ---- accuracy of the timed path vs FP64 (outside timing)
