@@ -254,7 +254,9 @@ int fcb200_trim(fcb200_handle h) {
     Buf* bufs[] = {&h->pos, &h->box, &h->masses, &h->pair_t, &h->pair_flag, &h->self_t, &h->psi_stage,
                    &h->phi_f32, &h->phi_hi, &h->phi_lo, &h->psi_hi, &h->psi_lo, &h->u1_hi, &h->u1_lo,
                    &h->u2_hi, &h->u2_lo, &h->u1_f32, &h->u2_f32, &h->psi_f32, &h->k3_stage[0],
-                   &h->k3_stage[1], &h->ifc2};
+                   &h->k3_stage[1], &h->ifc2, &h->sw_ints, &h->sw_nbr_r, &h->sw_pair_off, &h->sw_blk3,
+                   &h->sw_blk2, &h->sw_atoms, &h->sw_place, &h->sw_col_off, &h->sw_col_items, &h->sw_cursor,
+                   &h->sw_asr_off, &h->sw_asr_items, &h->sw_asr};
     for (Buf* b : bufs) b->release();
     return FCB_OK;
 }
@@ -392,6 +394,65 @@ int fcb200_second_order_lj(fcb200_handle h, const double* pos, int64_t N, const 
         return check_status(h, s);
     }
     return FCB_OK;
+}
+
+static int validate_sw(const double* pos, int64_t N, const double* box, double r_cut) {
+    if (pos == nullptr || box == nullptr) return set_error(FCB_ERR_ARG, "pos and box must not be NULL");
+    if (N < 1) return set_error(FCB_ERR_ARG, "n_atoms must be >= 1");
+    if (N > 4096) return set_error(FCB_ERR_ARG, "n_atoms > 4096 (dense n³ tensor would exceed device memory)");
+    if (!(r_cut > 0.0)) return set_error(FCB_ERR_ARG, "r_cut must be positive");
+    if (!(r_cut <= sw_potential_cutoff()))
+        return set_error(FCB_ERR_CUTOFF, "For AutoDiff SW silicon force constant cutoff must be less than potential cutoff");
+    return FCB_OK;
+}
+
+int fcb200_third_order_sw(fcb200_handle h, const double* pos, int64_t N, const double* box, double r_cut, double tol,
+                          const double* cos0, const double* masses, double* psi_out, float* psi32_mw_out, int flags,
+                          void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    FCB_TRY(validate_sw(pos, N, box, r_cut));
+    const bool weighted = (flags & FCB_PSI_MASS_WEIGHTED) != 0;
+    if ((weighted || psi32_mw_out) && !masses) return set_error(FCB_ERR_ARG, "masses are required for mass weighting");
+    if (!psi_out && !psi32_mw_out) return set_error(FCB_ERR_ARG, "no output buffer given");
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t n = 3 * N;
+    double *d_pos, *d_box, *d_m;
+    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
+    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
+    FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
+    const bool host64 = psi_out && !is_device_ptr(psi_out);
+    const bool host32 = psi32_mw_out && !is_device_ptr(psi32_mw_out);
+    if (host64) FCB_TRY(h->psi_stage.ensure(sizeof(double) * n * n * n));
+    if (host32) FCB_TRY(h->psi_f32.ensure(sizeof(float) * n * n * n));
+    AssemblyOut out;
+    out.psi64 = psi_out ? (host64 ? h->psi_stage.as<double>() : psi_out) : nullptr;
+    out.psi64_weighted = weighted;
+    out.psi32 = psi32_mw_out ? (host32 ? h->psi_f32.as<float>() : psi32_mw_out) : nullptr;
+    FCB_TRY(sw_third_order_launch(h, d_pos, N, d_box, r_cut, cos0, tol, d_m, out, s));
+    if (host64) FCB_CUDA(cudaMemcpyAsync(psi_out, out.psi64, sizeof(double) * n * n * n, cudaMemcpyDeviceToHost, s));
+    if (host32)
+        FCB_CUDA(cudaMemcpyAsync(psi32_mw_out, out.psi32, sizeof(float) * n * n * n, cudaMemcpyDeviceToHost, s));
+    return check_status(h, s);
+}
+
+int fcb200_second_order_sw(fcb200_handle h, const double* pos, int64_t N, const double* box, double r_cut,
+                           double tol, const double* cos0, const double* masses, double* ifc2_out, void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    FCB_TRY(validate_sw(pos, N, box, r_cut));
+    if (!ifc2_out) return set_error(FCB_ERR_ARG, "ifc2_out must not be NULL");
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t n = 3 * N;
+    double *d_pos, *d_box, *d_m, *d_out;
+    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
+    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
+    FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
+    FCB_TRY(device_view(h->ifc2, (const double*)ifc2_out, n * n, false, s, &d_out));
+    FCB_TRY(sw_second_order_launch(h, d_pos, N, d_box, r_cut, cos0, tol, d_m, d_out, s));
+    if (d_out != ifc2_out)
+        FCB_CUDA(cudaMemcpyAsync(ifc2_out, d_out, sizeof(double) * n * n, cudaMemcpyDeviceToHost, s));
+    return check_status(h, s);
 }
 
 static int mcc3_ranges_ok(int64_t n, int64_t a, int64_t b) { return 0 <= a && a < b && b <= n; }

@@ -73,6 +73,9 @@ struct fcb200_context {
     fcb::Buf psi_f32;               // staged Ψ (FP32) for host inputs
     fcb::Buf k3_stage[2];           // K3 staging slabs (device) for host outputs
     fcb::Buf ifc2;                  // second-order scratch
+    // Stillinger-Weber scratch (neighbours, blocks, placements, buckets, ASR rows)
+    fcb::Buf sw_ints, sw_nbr_r, sw_pair_off, sw_blk3, sw_blk2, sw_atoms, sw_place;
+    fcb::Buf sw_col_off, sw_col_items, sw_cursor, sw_asr_off, sw_asr_items, sw_asr;
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // Optional per-phase timing of fcb200_snapshot_lj (events on the caller's stream).
@@ -119,6 +122,15 @@ int ifc3_dense_write_raw(const double* T, const uint8_t* flag, const double* S, 
 int lj_second_order_launch(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box,
                            double sigma, double eps, double r_cut, double tol,
                            const double* d_masses, double* d_ifc2, cudaStream_t s);
+
+// Stillinger-Weber (sw_assembly.cu).  cos0 = {cosθ₀ of the generated blocks,
+// cosθ₀ of the iik block}, NULL for the reference's values.
+double sw_potential_cutoff();
+int sw_third_order_launch(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double r_cut,
+                          const double* cos0, double tol, const double* d_masses, const AssemblyOut& out,
+                          cudaStream_t s);
+int sw_second_order_launch(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double r_cut,
+                           const double* cos0, double tol, const double* d_masses, double* d_ifc2, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // mcc3 (mcc3.cu, mode_product_simt.cu, mode_product_tc.cu)

@@ -1,0 +1,872 @@
+// Stillinger-Weber silicon IFC2/IFC3 assembly on sm_100a.
+//
+// Reference semantics (ForceConstants.jl, AutoDiffCalculator):
+//   third_order!(IFC3, sys, ::StillingerWeberSilicon, ::AutoDiffCalculator)
+//                                   src/autodiff/third_order_AD.jl:71-170
+//   set_third_order_terms!/_alt!    src/autodiff/third_order_AD.jl:180-224
+//   second_order! (SW)              src/autodiff/second_order_AD.jl:40-110
+//   Φ₂, Φ₃_si, parameters           src/interactions/SW.jl:29-83
+//   ASR!, apply_tols!               src/asr.jl:3-40, src/helper_funcs.jl:20-27
+//
+// The reference walks centre atoms i, partners j ≠ i and k > j inside the
+// cutoff, evaluates automatically generated third-derivative blocks of the pair
+// term Φ₂(|r_ij|) and of the three-body term h(r_i, r_j, r_k) =
+// λϵ (cosθ_jik − cosθ₀)² exp(γσ/(r_ij−aσ)) exp(γσ/(r_ik−aσ)), and scatters each
+// block into up to six permuted positions of the dense Ψ with `+=`; ASR! then
+// overwrites every (x,y,x) block.  The generated blocks carry cosθ₀ written as
+// −0.333333333333 while the iik block is built at run time from the exact −1/3;
+// both values are parameters here (cos0_gen, cos0_iik).
+//
+// Device pipeline (all kernels in this file):
+//   1. neighbour lists (single minimum image, strict cutoff test as the reference);
+//   2. triplet and pair enumeration (exclusive scans);
+//   3. analytic derivative blocks: h depends on u = r_i − r_j and v = r_i − r_k
+//      only; its third derivatives in (u,v) are built by the product and chain
+//      rules from closed-form derivatives of the radial factors exp(γσ/(r−aσ))
+//      and 1/r and of the bilinear u·v, then contracted with the atom Jacobians
+//      (∂_i = ∂_u + ∂_v, ∂_j = −∂_u, ∂_k = −∂_v) into the seven blocks the
+//      reference uses; the pair block uses the radial third-derivative formula
+//      of Φ₂;
+//   4. "placements": every (block, permutation, sign, target atom triple) the
+//      reference's scatter would add, with the reference's loop order as key;
+//   5. deterministic buckets: placements grouped by target column (Y,Z) and by
+//      ASR row (X,Y), each bucket sorted by (atom, loop order), so every Ψ
+//      entry is summed in the same order as the reference accumulates it;
+//   6. the dense writer: one warp per column of Ψ, like the LJ writer, with
+//      the ASR entries taken from the (X,Y) buckets.
+#include "fcb200_internal.cuh"
+
+namespace fcb {
+namespace {
+
+constexpr int MAXNB = 16;  // neighbour capacity per atom (diamond Si: 4)
+
+struct SwPot {
+    double eps, sigma, a, lambda, gamma, A, B;
+    double rc, gs, le;  // aσ, σγ, ϵλ (SW.jl:38-40)
+    double cos0_gen, cos0_iik;
+};
+
+__device__ __forceinline__ void nearest_mirror(double r[3], const double* box) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double L = box[d];
+        if (r[d] > L / 2.0) r[d] = r[d] - L;
+        else if (r[d] < -L / 2.0) r[d] = r[d] + L;
+    }
+}
+
+// 1. neighbour lists, ascending partner index (the reference's j loop order).
+__global__ void sw_neighbor_kernel(const double* __restrict__ pos, const double* __restrict__ box, int N, double rc2,
+                                   int* __restrict__ nbr, double* __restrict__ nbr_r, int* __restrict__ cnt,
+                                   int* __restrict__ ntrip, int* __restrict__ npair, int* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int c = 0, up = 0;
+    for (int j = 0; j < N; ++j) {
+        if (j == i) continue;
+        double r[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) r[d] = __dsub_rn(pos[3 * i + d], pos[3 * j + d]);
+        nearest_mirror(r, box);
+        const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(r[0], r[0]), __dmul_rn(r[1], r[1])), __dmul_rn(r[2], r[2]));
+        if (!(d2 < rc2)) continue;
+        if (c < MAXNB) {
+            nbr[i * MAXNB + c] = j;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) nbr_r[(i * MAXNB + c) * 3 + d] = r[d];
+        }
+        ++c;
+        if (j > i) ++up;
+    }
+    if (c > MAXNB) {
+        atomicCAS(status, 0, 100 + MAXNB);
+        c = MAXNB;
+    }
+    cnt[i] = c;
+    ntrip[i] = c * (c - 1) / 2;
+    npair[i] = up;
+}
+
+// Exclusive scan of `len` ints by one CTA (out has len + 1 entries).
+__global__ void scan_kernel(const int* __restrict__ in, int64_t len, int* __restrict__ out) {
+    __shared__ int part[1024];
+    const int t = threadIdx.x, T = blockDim.x;
+    const int64_t chunk = (len + T - 1) / T;
+    const int64_t b = t * chunk, e = b + chunk < len ? b + chunk : len;
+    int s = 0;
+    for (int64_t i = b; i < e; ++i) s += in[i];
+    part[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        int acc = 0;
+        for (int i = 0; i < T; ++i) {
+            const int v = part[i];
+            part[i] = acc;
+            acc += v;
+        }
+        out[len] = acc;
+    }
+    __syncthreads();
+    int acc = part[t];
+    for (int64_t i = b; i < e; ++i) {
+        out[i] = acc;
+        acc += in[i];
+    }
+}
+
+__device__ __forceinline__ int find_owner(const int* __restrict__ off, int N, int t) {
+    int lo = 0, hi = N;  // largest i with off[i] <= t
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------- jets
+// 6-variable jet x = (u0,u1,u2,v0,v1,v2): [0] value, [1+α] gradient,
+// [7+6α+β] Hessian, [43+36α+6β+γ] third derivatives.  3-variable jets of a
+// radial factor: [0] value, [1+a], [4+3a+b], [13+9a+3b+c].
+constexpr int J6 = 259, J3 = 40;
+constexpr int G1 = 1, H1 = 7, T1 = 43;
+
+// radial jet of f(|x|) in 3 variables from f, f', f'', f''' (one entry per call)
+__device__ double radial_entry(int e, double f, double f1, double f2, double f3, const double xh[3], double r) {
+    if (e == 0) return f;
+    if (e < 4) return f1 * xh[e - 1];
+    if (e < 13) {
+        const int a = (e - 4) / 3, b = (e - 4) % 3;
+        return f2 * xh[a] * xh[b] + (f1 / r) * ((a == b ? 1.0 : 0.0) - xh[a] * xh[b]);
+    }
+    const int q = e - 13, a = q / 9, b = (q / 3) % 3, c = q % 3;
+    const double k = f2 / r - f1 / (r * r);
+    const double d = (a == b ? xh[c] : 0.0) + (a == c ? xh[b] : 0.0) + (b == c ? xh[a] : 0.0);
+    return f3 * xh[a] * xh[b] * xh[c] + k * (d - 3.0 * xh[a] * xh[b] * xh[c]);
+}
+
+// entry e of the 6-variable jet of F(u)·H(v)
+__device__ double embed_entry(int e, const double* F, const double* H) {
+    if (e == 0) return F[0] * H[0];
+    if (e < H1) {
+        const int al = e - G1;
+        return al < 3 ? F[1 + al] * H[0] : F[0] * H[1 + al - 3];
+    }
+    if (e < T1) {
+        const int q = e - H1, al = q / 6, be = q % 6;
+        const bool ua = al < 3, ub = be < 3;
+        if (ua && ub) return F[4 + 3 * al + be] * H[0];
+        if (!ua && !ub) return F[0] * H[4 + 3 * (al - 3) + (be - 3)];
+        return ua ? F[1 + al] * H[1 + be - 3] : F[1 + be] * H[1 + al - 3];
+    }
+    const int q = e - T1, idx[3] = {q / 36, (q / 6) % 6, q % 6};
+    int us[3], vs[3], nu = 0, nv = 0;
+    for (int m = 0; m < 3; ++m) {
+        if (idx[m] < 3) us[nu++] = idx[m];
+        else vs[nv++] = idx[m] - 3;
+    }
+    double fu = 0.0, hv = 0.0;
+    if (nu == 0) fu = F[0];
+    else if (nu == 1) fu = F[1 + us[0]];
+    else if (nu == 2) fu = F[4 + 3 * us[0] + us[1]];
+    else fu = F[13 + 9 * us[0] + 3 * us[1] + us[2]];
+    if (nv == 0) hv = H[0];
+    else if (nv == 1) hv = H[1 + vs[0]];
+    else if (nv == 2) hv = H[4 + 3 * vs[0] + vs[1]];
+    else hv = H[13 + 9 * vs[0] + 3 * vs[1] + vs[2]];
+    return fu * hv;
+}
+
+// entry e of the jet of the product A·B (Leibniz rule)
+__device__ double product_entry(int e, const double* A, const double* B) {
+    if (e == 0) return A[0] * B[0];
+    if (e < H1) {
+        const int al = e - G1;
+        return A[G1 + al] * B[0] + A[0] * B[G1 + al];
+    }
+    if (e < T1) {
+        const int q = e - H1, al = q / 6, be = q % 6;
+        return A[H1 + q] * B[0] + A[G1 + al] * B[G1 + be] + A[G1 + be] * B[G1 + al] + A[0] * B[H1 + q];
+    }
+    const int q = e - T1, al = q / 36, be = (q / 6) % 6, ga = q % 6;
+    const int ab = 6 * al + be, ag = 6 * al + ga, bg = 6 * be + ga;
+    return A[T1 + q] * B[0] + A[H1 + ab] * B[G1 + ga] + A[H1 + ag] * B[G1 + be] + A[H1 + bg] * B[G1 + al] +
+           A[G1 + al] * B[H1 + bg] + A[G1 + be] * B[H1 + ag] + A[G1 + ga] * B[H1 + ab] + A[0] * B[T1 + q];
+}
+
+// entry e of the jet of g(C) with g = (C − c0)²: g' = 2(C − c0), g'' = 2, g''' = 0
+__device__ double square_entry(int e, const double* C, double c0) {
+    const double d = C[0] - c0, g1 = 2.0 * d;
+    if (e == 0) return d * d;
+    if (e < H1) return g1 * C[e];
+    if (e < T1) {
+        const int q = e - H1, al = q / 6, be = q % 6;
+        return 2.0 * C[G1 + al] * C[G1 + be] + g1 * C[e];
+    }
+    const int q = e - T1, al = q / 36, be = (q / 6) % 6, ga = q % 6;
+    return 2.0 * (C[H1 + 6 * al + be] * C[G1 + ga] + C[H1 + 6 * al + ga] * C[G1 + be] +
+                  C[H1 + 6 * be + ga] * C[G1 + al]) +
+           g1 * C[e];
+}
+
+// jet of w = u·v
+__device__ double dot_entry(int e, const double u[3], const double v[3]) {
+    if (e == 0) return u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+    if (e < H1) {
+        const int al = e - G1;
+        return al < 3 ? v[al] : u[al - 3];
+    }
+    if (e < T1) {
+        const int q = e - H1, al = q / 6, be = q % 6;
+        if (al < 3 && be >= 3) return al == be - 3 ? 1.0 : 0.0;
+        if (al >= 3 && be < 3) return al - 3 == be ? 1.0 : 0.0;
+        return 0.0;
+    }
+    return 0.0;
+}
+
+struct RadialScalars {
+    double f, f1, f2, f3;
+};
+
+// exp(s/(r − rc)) and its derivatives
+__device__ RadialScalars exp_radial(double r, double s, double rc) {
+    const double t = r - rc, q = s / t, e = exp(q);
+    const double q1 = -s / (t * t), q2 = 2.0 * s / (t * t * t), q3 = -6.0 * s / (t * t * t * t);
+    return {e, e * q1, e * (q1 * q1 + q2), e * (q1 * q1 * q1 + 3.0 * q1 * q2 + q3)};
+}
+
+__device__ RadialScalars inv_radial(double r) {
+    const double i = 1.0 / r;
+    return {i, -i * i, 2.0 * i * i * i, -6.0 * i * i * i * i};
+}
+
+// Φ₂(r) = Aϵ (B (σ/r)^4 − 1) exp(σ/(r − aσ)) and its derivatives (SW.jl:76-78, q = 0)
+__device__ RadialScalars phi2_radial(double r, const SwPot& P) {
+    const double sr = P.sigma / r, s4 = sr * sr * sr * sr;
+    const double S = P.B * s4 - 1.0, S1 = -4.0 * P.B * s4 / r, S2 = 20.0 * P.B * s4 / (r * r),
+                 S3 = -120.0 * P.B * s4 / (r * r * r);
+    const RadialScalars X = exp_radial(r, P.sigma, P.rc);
+    const double C = P.A * P.eps;
+    return {C * S * X.f, C * (S1 * X.f + S * X.f1), C * (S2 * X.f + 2.0 * S1 * X.f1 + S * X.f2),
+            C * (S3 * X.f + 3.0 * S2 * X.f1 + 3.0 * S1 * X.f2 + S * X.f3)};
+}
+
+// 3. one warp per triplet: the seven IFC3 blocks and the three IFC2 blocks.
+constexpr int TRIP_WARPS = 4;
+__global__ void __launch_bounds__(32 * TRIP_WARPS)
+    sw_triplet_kernel(const double* __restrict__ pos, int N, const int* __restrict__ nbr,
+                      const double* __restrict__ nbr_r, const int* __restrict__ cnt, const int* __restrict__ trip_off,
+                      int n_trip, SwPot P, double* __restrict__ blk3, double* __restrict__ blk2,
+                      int4* __restrict__ trip_atoms) {
+    __shared__ double sm[TRIP_WARPS][4 * J3 + 5 * J6];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * TRIP_WARPS + w;
+    if (t >= n_trip) return;
+    double* Eu = sm[w];
+    double* Ev = Eu + J3;
+    double* Pu = Ev + J3;
+    double* Qv = Pu + J3;
+    double* R = Qv + J3;   // (1/|u|)(1/|v|)
+    double* Cj = R + J6;   // cosθ
+    double* Pe = Cj + J6;  // E(|u|) E(|v|)
+    double* Gj = Pe + J6;  // (cosθ − c0)²
+    double* Hh = Gj + J6;  // h / λϵ
+
+    const int i = find_owner(trip_off, N, t);
+    const int c = cnt[i];
+    int q = t - trip_off[i], js = 0;
+    while (q >= c - 1 - js) q -= c - 1 - js, ++js;
+    const int ks = js + 1 + q;
+    const int j = nbr[i * MAXNB + js], k = nbr[i * MAXNB + ks];
+    // the reference's r_arr = [r_i; r_i − r_ij; r_i − r_ik] (third_order_AD.jl:122-125)
+    double u[3], v[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double xi = pos[3 * i + d];
+        const double xj = xi - nbr_r[(i * MAXNB + js) * 3 + d];
+        const double xk = xi - nbr_r[(i * MAXNB + ks) * 3 + d];
+        u[d] = xi - xj;
+        v[d] = xi - xk;
+    }
+    const double ru = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double rv = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const double uh[3] = {u[0] / ru, u[1] / ru, u[2] / ru}, vh[3] = {v[0] / rv, v[1] / rv, v[2] / rv};
+    const RadialScalars eu = exp_radial(ru, P.gs, P.rc), ev = exp_radial(rv, P.gs, P.rc);
+    const RadialScalars pu = inv_radial(ru), qv = inv_radial(rv);
+    for (int e = lane; e < J3; e += 32) {
+        Eu[e] = radial_entry(e, eu.f, eu.f1, eu.f2, eu.f3, uh, ru);
+        Ev[e] = radial_entry(e, ev.f, ev.f1, ev.f2, ev.f3, vh, rv);
+        Pu[e] = radial_entry(e, pu.f, pu.f1, pu.f2, pu.f3, uh, ru);
+        Qv[e] = radial_entry(e, qv.f, qv.f1, qv.f2, qv.f3, vh, rv);
+    }
+    __syncwarp();
+    for (int e = lane; e < J6; e += 32) {
+        R[e] = embed_entry(e, Pu, Qv);
+        Pe[e] = embed_entry(e, Eu, Ev);
+    }
+    __syncwarp();
+    // C = w · R, with w's jet generated on the fly into Gj as scratch
+    for (int e = lane; e < J6; e += 32) Gj[e] = dot_entry(e, u, v);
+    __syncwarp();
+    for (int e = lane; e < J6; e += 32) Cj[e] = product_entry(e, Gj, R);
+    __syncwarp();
+    for (int pass = 0; pass < 2; ++pass) {
+        const double c0 = pass == 0 ? P.cos0_gen : P.cos0_iik;
+        for (int e = lane; e < J6; e += 32) Gj[e] = square_entry(e, Cj, c0);
+        __syncwarp();
+        for (int e = lane; e < J6; e += 32) Hh[e] = P.le * product_entry(e, Gj, Pe);
+        __syncwarp();
+        // contraction with the atom Jacobians; T(s,a; t,b; w,c) with s,t,w ∈ {u:0, v:1}
+        auto T3 = [&](int s, int a, int tt, int b, int ww, int cc) {
+            return Hh[T1 + 36 * (3 * s + a) + 6 * (3 * tt + b) + 3 * ww + cc];
+        };
+        double* out = blk3 + (int64_t)t * 7 * 27;
+        for (int e = lane; e < 27; e += 32) {
+            const int a = e % 3, b = (e / 3) % 3, cc = e / 9;  // block[a,b,c] at a + 3b + 9c
+            if (pass == 0) {
+                out[0 * 27 + e] = -(T3(0, a, 0, b, 0, cc) + T3(0, a, 1, b, 0, cc) + T3(1, a, 0, b, 0, cc) +
+                                    T3(1, a, 1, b, 0, cc));                              // iij
+                out[1 * 27 + e] = T3(0, a, 0, b, 0, cc) + T3(1, a, 0, b, 0, cc);         // ijj
+                out[3 * 27 + e] = T3(0, a, 1, b, 1, cc) + T3(1, a, 1, b, 1, cc);         // ikk
+                out[4 * 27 + e] = -T3(0, a, 0, b, 1, cc);                                // jjk
+                out[5 * 27 + e] = -T3(0, a, 1, b, 1, cc);                                // jkk
+                out[6 * 27 + e] = T3(0, a, 0, b, 1, cc) + T3(1, a, 0, b, 1, cc);         // ijk
+            } else {
+                out[2 * 27 + e] = -(T3(0, a, 0, b, 1, cc) + T3(0, a, 1, b, 1, cc) + T3(1, a, 0, b, 1, cc) +
+                                    T3(1, a, 1, b, 1, cc));                              // iik
+            }
+        }
+        if (pass == 0) {
+            double* o2 = blk2 + (int64_t)t * 27;
+            for (int e = lane; e < 9; e += 32) {
+                const int a = e % 3, b = e / 3;  // block[a,b] at a + 3b
+                auto H2 = [&](int s, int aa, int tt, int bb) { return Hh[H1 + 6 * (3 * s + aa) + 3 * tt + bb]; };
+                o2[e] = -(H2(0, a, 0, b) + H2(1, a, 0, b));       // ij: (∂u+∂v)_a (−∂u)_b
+                o2[9 + e] = -(H2(0, a, 1, b) + H2(1, a, 1, b));   // ik
+                o2[18 + e] = H2(0, a, 1, b);                      // jk: (−∂u)_a (−∂v)_b
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0) trip_atoms[t] = make_int4(i, j, k, 0);
+}
+
+// pair blocks: H3 and H2 of Φ₂(|r_ij|) for every pair i < j inside the cutoff
+__global__ void sw_pair_kernel(int N, const int* __restrict__ nbr, const double* __restrict__ nbr_r,
+                               const int* __restrict__ cnt, const int* __restrict__ pair_off, int n_pair, SwPot P,
+                               double* __restrict__ pblk3, double* __restrict__ pblk2, int2* __restrict__ pair_atoms) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_pair) return;
+    const int i = find_owner(pair_off, N, p);
+    int q = p - pair_off[i], s = 0;
+    for (; s < cnt[i]; ++s)
+        if (nbr[i * MAXNB + s] > i && q-- == 0) break;
+    const int j = nbr[i * MAXNB + s];
+    const double* r = nbr_r + (i * MAXNB + s) * 3;
+    const double rn = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    const double xh[3] = {r[0] / rn, r[1] / rn, r[2] / rn};
+    const RadialScalars f = phi2_radial(rn, P);
+    for (int e = 0; e < 27; ++e) pblk3[(int64_t)p * 27 + e] = radial_entry(13 + 9 * (e / 9) + 3 * ((e / 3) % 3) + e % 3,
+                                                                            f.f, f.f1, f.f2, f.f3, xh, rn);
+    for (int e = 0; e < 9; ++e) pblk2[(int64_t)p * 9 + e] = radial_entry(4 + 3 * (e / 3) + e % 3, f.f, f.f1, f.f2, f.f3, xh, rn);
+    pair_atoms[p] = make_int2(i, j);
+}
+
+// ------------------------------------------------------------ placements
+// perm codes: 0 id [a,b,c]; 1 (1,3,2) → [a,c,b]; 2 (3,2,1) → [c,b,a];
+//             3 (2,1,3) → [b,a,c]; 4 (2,3,1) → [c,a,b]; 5 (3,1,2) → [b,c,a]
+// (Julia permutedims semantics, third_order_AD.jl:194-224).
+struct Place {
+    int x, y, z;
+    int src;   // block index (27 doubles, or 9 for IFC2 placements)
+    int code;  // perm | (negate << 3)
+    int pad;
+    long long order;
+};
+
+__device__ __forceinline__ int perm_index(int code, int a, int b, int c) {
+    switch (code & 7) {
+        case 0: return a + 3 * b + 9 * c;
+        case 1: return a + 3 * c + 9 * b;
+        case 2: return c + 3 * b + 9 * a;
+        case 3: return b + 3 * a + 9 * c;
+        case 4: return c + 3 * a + 9 * b;
+        default: return b + 3 * c + 9 * a;
+    }
+}
+
+__device__ __forceinline__ long long loop_order(int i, int j, int k_plus1, int slot, int N) {
+    return (((long long)i * N + j) * (N + 1) + k_plus1) * 32 + slot;
+}
+
+__global__ void sw_place3_kernel(const int4* __restrict__ trip_atoms, int n_trip, const int2* __restrict__ pair_atoms,
+                                 int n_pair, int N, Place* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n_trip) {
+        const int4 a = trip_atoms[t];
+        const int i = a.x, j = a.y, k = a.z;
+        // (target x,y,z, block, perm) in the reference's scatter sequence
+        const int tab[24][5] = {{i, i, j, 0, 0}, {i, j, i, 0, 1}, {j, i, i, 0, 2},   // iij (aab)
+                                {i, j, j, 1, 0}, {j, i, j, 1, 3}, {j, j, i, 1, 2},   // ijj (abb)
+                                {i, i, k, 2, 0}, {i, k, i, 2, 1}, {k, i, i, 2, 2},   // iik (aab)
+                                {i, k, k, 3, 0}, {k, i, k, 3, 3}, {k, k, i, 3, 2},   // ikk (abb)
+                                {j, j, k, 4, 0}, {j, k, j, 4, 1}, {k, j, j, 4, 2},   // jjk (aab)
+                                {j, k, k, 5, 0}, {k, j, k, 5, 3}, {k, k, j, 5, 2},   // jkk (abb)
+                                {i, j, k, 6, 0}, {i, k, j, 6, 1}, {j, i, k, 6, 3},   // ijk (abc)
+                                {j, k, i, 6, 4}, {k, i, j, 6, 5}, {k, j, i, 6, 2}};
+        for (int s = 0; s < 24; ++s) {
+            Place p;
+            p.x = tab[s][0];
+            p.y = tab[s][1];
+            p.z = tab[s][2];
+            p.src = t * 7 + tab[s][3];
+            p.code = tab[s][4];
+            p.pad = 0;
+            p.order = loop_order(i, j, k + 1, s, N);
+            out[(int64_t)t * 24 + s] = p;
+        }
+    } else if (t < n_trip + n_pair) {
+        const int q = t - n_trip;
+        const int2 a = pair_atoms[q];
+        const int i = a.x, j = a.y;
+        // set_third_order_terms!(IFC3, i, j, -block); set_third_order_terms!(IFC3, j, i, block)
+        const int tab[6][4] = {{i, i, j, 1}, {i, j, i, 1}, {j, i, i, 1}, {j, j, i, 0}, {j, i, j, 0}, {i, j, j, 0}};
+        for (int s = 0; s < 6; ++s) {
+            Place p;
+            p.x = tab[s][0];
+            p.y = tab[s][1];
+            p.z = tab[s][2];
+            p.src = n_trip * 7 + q;
+            p.code = tab[s][3] << 3;
+            p.pad = 0;
+            p.order = loop_order(i, j, 0, s, N);
+            out[(int64_t)n_trip * 24 + (int64_t)q * 6 + s] = p;
+        }
+    }
+}
+
+// IFC2 placements (second_order_AD.jl:57-95): triplet ij, ik, jk blocks and
+// their transposes; pair −H2 to (i,j) and (j,i).
+__global__ void sw_place2_kernel(const int4* __restrict__ trip_atoms, int n_trip, const int2* __restrict__ pair_atoms,
+                                 int n_pair, int N, Place* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n_trip) {
+        const int4 a = trip_atoms[t];
+        const int i = a.x, j = a.y, k = a.z;
+        const int tab[6][4] = {{i, j, 0, 0}, {j, i, 0, 3}, {i, k, 1, 0}, {k, i, 1, 3}, {j, k, 2, 0}, {k, j, 2, 3}};
+        for (int s = 0; s < 6; ++s) {
+            Place p;
+            p.x = tab[s][0];
+            p.y = tab[s][1];
+            p.z = -1;
+            p.src = t * 3 + tab[s][2];
+            p.code = tab[s][3];
+            p.pad = 0;
+            p.order = loop_order(i, j, k + 1, s, N);
+            out[(int64_t)t * 6 + s] = p;
+        }
+    } else if (t < n_trip + n_pair) {
+        const int q = t - n_trip;
+        const int2 a = pair_atoms[q];
+        for (int s = 0; s < 2; ++s) {
+            Place p;
+            p.x = s == 0 ? a.x : a.y;
+            p.y = s == 0 ? a.y : a.x;
+            p.z = -1;
+            p.src = n_trip * 3 + q;
+            p.code = 1 << 3;
+            p.pad = 0;
+            p.order = loop_order(a.x, a.y, 0, s, N);
+            out[(int64_t)n_trip * 6 + (int64_t)q * 2 + s] = p;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- buckets
+// kind 0: IFC3 columns, key (y,z), sorted by (x, order)
+// kind 1: IFC3 ASR rows, key (x,y), only z != x, sorted by (z, order)
+// kind 2: IFC2 entries, key (x,y), sorted by order
+__device__ __forceinline__ bool bucket_of(const Place& p, int kind, int N, int* key) {
+    if (kind == 0) {
+        *key = p.y * N + p.z;
+        return true;
+    }
+    if (kind == 1) {
+        if (p.z == p.x) return false;
+        *key = p.x * N + p.y;
+        return true;
+    }
+    *key = p.x * N + p.y;
+    return true;
+}
+
+__device__ __forceinline__ long long sort_key(const Place& p, int kind) {
+    const long long lo = p.order & ((1LL << 40) - 1);
+    if (kind == 0) return ((long long)p.x << 40) | lo;
+    if (kind == 1) return ((long long)p.z << 40) | lo;
+    return lo;
+}
+
+__global__ void bucket_count_kernel(const Place* __restrict__ pl, int n, int kind, int N, int* __restrict__ cnt) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int key;
+    if (bucket_of(pl[t], kind, N, &key)) atomicAdd(&cnt[key], 1);
+}
+
+__global__ void bucket_fill_kernel(const Place* __restrict__ pl, int n, int kind, int N, int* __restrict__ cursor,
+                                   int* __restrict__ items) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int key;
+    if (bucket_of(pl[t], kind, N, &key)) items[atomicAdd(&cursor[key], 1)] = t;
+}
+
+__global__ void bucket_sort_kernel(const Place* __restrict__ pl, int kind, int nb, const int* __restrict__ off,
+                                   int* __restrict__ items) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const int s = off[b], e = off[b + 1];
+    for (int x = s + 1; x < e; ++x) {  // insertion sort: deterministic order
+        const int it = items[x];
+        const long long k = sort_key(pl[it], kind);
+        int y = x - 1;
+        while (y >= s && sort_key(pl[items[y]], kind) > k) {
+            items[y + 1] = items[y];
+            --y;
+        }
+        items[y + 1] = it;
+    }
+}
+
+__device__ __forceinline__ double place_value3(const Place& p, const double* __restrict__ blocks, int a, int b, int c) {
+    const double v = blocks[(int64_t)p.src * 27 + perm_index(p.code, a, b, c)];
+    return (p.code >> 3) ? -v : v;
+}
+
+// ASR rows: S[x,y][a,b,c] = −Σ_{z ≠ x, ascending} Ψ[x a, y b, z c]  (asr.jl:31-32)
+__global__ void sw_asr3_kernel(const Place* __restrict__ pl, const double* __restrict__ blocks, int NN,
+                               const int* __restrict__ off, const int* __restrict__ items, double* __restrict__ S) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)NN * 27) return;
+    const int b = (int)(t / 27), comp = (int)(t % 27);
+    const int s = off[b], e = off[b + 1];
+    if (s == e) return;
+    const int a = comp % 3, bb = (comp / 3) % 3, c = comp / 9;
+    double total = 0.0, group = 0.0;
+    int zcur = pl[items[s]].z;
+    for (int q = s; q < e; ++q) {
+        const Place p = pl[items[q]];
+        if (p.z != zcur) {
+            total += group;
+            group = 0.0;
+            zcur = p.z;
+        }
+        group += place_value3(p, blocks, a, bb, c);
+    }
+    total += group;
+    S[t] = -total;
+}
+
+struct SwDense {
+    int N, n;
+    int64_t n_pad;
+    double tol;
+    const Place* pl;
+    const double* blocks;
+    const int* col_off;
+    const int* col_items;
+    const int* asr_off;
+    const double* S;
+    const double* masses;
+    double* psi64;
+    bool psi64_weighted;
+    float* psi32;
+    void* split_hi;
+    void* split_lo;
+    int split_kind;
+};
+
+__device__ __forceinline__ double sw_finish(const SwDense& g, double v, int I, int J, int K, double* mw) {
+    if (fabs(v) < g.tol) v = 0.0;
+    if (g.masses != nullptr && v != 0.0)
+        *mw = v / sqrt((g.masses[I] * g.masses[J]) * g.masses[K]);
+    else
+        *mw = v;
+    return v;
+}
+
+// Ψ[I a, J b, K c] before tol
+__device__ double sw_value(const SwDense& g, int I, int a, int J, int b, int K, int c, int s, int e) {
+    if (I == K) {
+        const int bk = K * g.N + J;
+        return g.asr_off[bk] == g.asr_off[bk + 1] ? 0.0 : g.S[(int64_t)bk * 27 + a + 3 * b + 9 * c];
+    }
+    // bucket [s,e) is sorted by target x: binary search for x == I
+    int lo = s, hi = e;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (g.pl[g.col_items[mid]].x < I) lo = mid + 1;
+        else hi = mid;
+    }
+    double v = 0.0;
+    for (int q = lo; q < e; ++q) {
+        const Place p = g.pl[g.col_items[q]];
+        if (p.x != I) break;
+        v += place_value3(p, g.blocks, a, b, c);
+    }
+    return v;
+}
+
+__device__ __forceinline__ void sw_store(const SwDense& g, int64_t col, int e, double r, double w) {
+    if (g.psi64) g.psi64[col * g.n + e] = g.psi64_weighted ? w : r;
+    if (g.psi32) g.psi32[col * g.n + e] = (float)w;
+    const int64_t off = col * g.n_pad + e;
+    if (g.split_kind == 1) {
+        const __nv_bfloat16 h = __float2bfloat16_rn((float)w);
+        static_cast<__nv_bfloat16*>(g.split_hi)[off] = h;
+        static_cast<__nv_bfloat16*>(g.split_lo)[off] = __float2bfloat16_rn((float)(w - (double)__bfloat162float(h)));
+    } else if (g.split_kind == 2) {
+        uint32_t hb;
+        const float f = (float)w;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(f));
+        const float h = __uint_as_float(hb);
+        static_cast<float*>(g.split_hi)[off] = h;
+        static_cast<float*>(g.split_lo)[off] = (float)(w - (double)h);
+    }
+}
+
+// one warp per column (jj,kk); lanes over the rows
+__global__ void __launch_bounds__(256) sw_dense_kernel(SwDense g) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int n = g.n, N = g.N;
+    for (int64_t col = warp; col < (int64_t)n * n; col += nwarps) {
+        const int kk = (int)(col / n), jj = (int)(col - (int64_t)kk * n);
+        const int J = jj / 3, K = kk / 3, b = jj - 3 * J, c = kk - 3 * K;
+        const int cb = J * N + K, s = g.col_off[cb], e = g.col_off[cb + 1];
+        const int ab = K * N + J;
+        const bool asr_live = g.asr_off[ab] != g.asr_off[ab + 1];
+        const bool live = (s != e) || asr_live;
+        for (int r = lane; r < n; r += 32) {
+            double raw = 0.0, mw = 0.0;
+            if (live) {
+                const int I = r / 3, a = r - 3 * I;
+                raw = sw_finish(g, sw_value(g, I, a, J, b, K, c, s, e), I, J, K, &mw);
+            }
+            sw_store(g, col, r, raw, mw);
+        }
+    }
+}
+
+// IFC2 (second_order_AD.jl:40-110 + asr.jl:3-17 + apply_tols!), optional 1/sqrt(m_i m_j)
+__global__ void sw_ifc2_kernel(int N, double tol, const Place* __restrict__ pl, const double* __restrict__ blocks2,
+                               const int* __restrict__ off, const int* __restrict__ items,
+                               const double* __restrict__ masses, double* __restrict__ out) {
+    const int n = 3 * N;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)n * n) return;
+    const int ii = (int)(t % n), jj = (int)(t / n);
+    const int I = ii / 3, J = jj / 3, a = ii - 3 * I, b = jj - 3 * J;
+    auto entry = [&](int X, int Y) {
+        const int bk = X * N + Y;
+        double v = 0.0;
+        for (int q = off[bk]; q < off[bk + 1]; ++q) {
+            const Place p = pl[items[q]];
+            const double x = blocks2[(int64_t)p.src * 9 + ((p.code & 7) == 3 ? b + 3 * a : a + 3 * b)];
+            v += (p.code >> 3) ? -x : x;
+        }
+        return v;
+    };
+    double v;
+    if (I != J) {
+        v = entry(I, J);
+    } else {
+        double s = 0.0;
+        for (int Y = 0; Y < N; ++Y)
+            if (Y != I) s += entry(I, Y);
+        v = -1.0 * s;
+    }
+    if (fabs(v) < tol) v = 0.0;
+    if (masses != nullptr) v = v / sqrt(masses[I] * masses[J]);
+    out[t] = v;
+}
+
+}  // namespace
+
+// Host driver shared by the IFC3 and IFC2 entry points.
+struct SwWork {
+    int N, n_trip, n_pair;
+    int *nbr, *cnt, *ntrip, *npair, *trip_off, *pair_off;
+    double* nbr_r;
+    double *blk3, *blk2;
+    int4* trip_atoms;
+    int2* pair_atoms;
+};
+
+static int sw_prepare(fcb200_context* h, const double* d_pos, int N, const double* d_box, double r_cut, SwPot P,
+                      cudaStream_t s, SwWork* W) {
+    (void)P;
+    W->N = N;
+    const size_t ints = (size_t)N * MAXNB + 4 * (size_t)(N + 1);
+    FCB_TRY(h->sw_ints.ensure(sizeof(int) * ints));
+    FCB_TRY(h->sw_nbr_r.ensure(sizeof(double) * 3 * N * MAXNB));
+    int* base = h->sw_ints.as<int>();
+    W->nbr = base;
+    W->cnt = base + (size_t)N * MAXNB;
+    W->ntrip = W->cnt + (N + 1);
+    W->npair = W->ntrip + (N + 1);
+    W->trip_off = W->npair + (N + 1);
+    FCB_TRY(h->sw_pair_off.ensure(sizeof(int) * (N + 1)));
+    W->pair_off = h->sw_pair_off.as<int>();
+    W->nbr_r = h->sw_nbr_r.as<double>();
+    sw_neighbor_kernel<<<(N + 127) / 128, 128, 0, s>>>(d_pos, d_box, N, r_cut * r_cut, W->nbr, W->nbr_r, W->cnt,
+                                                       W->ntrip, W->npair, h->d_status);
+    FCB_CUDA(cudaGetLastError());
+    scan_kernel<<<1, 1024, 0, s>>>(W->ntrip, N, W->trip_off);
+    scan_kernel<<<1, 1024, 0, s>>>(W->npair, N, W->pair_off);
+    FCB_CUDA(cudaGetLastError());
+    int tot[2];
+    FCB_CUDA(cudaMemcpyAsync(&tot[0], W->trip_off + N, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FCB_CUDA(cudaMemcpyAsync(&tot[1], W->pair_off + N, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FCB_CUDA(cudaStreamSynchronize(s));
+    int st = 0;
+    FCB_CUDA(cudaMemcpy(&st, h->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st >= 100) {
+        int zero = 0;
+        cudaMemcpy(h->d_status, &zero, sizeof(int), cudaMemcpyHostToDevice);
+        return set_error(FCB_ERR_ARG, "an atom has more than " + std::to_string(MAXNB) +
+                                          " neighbours inside the Stillinger-Weber cutoff");
+    }
+    W->n_trip = tot[0];
+    W->n_pair = tot[1];
+    FCB_TRY(h->sw_blk3.ensure(sizeof(double) * 27 * ((size_t)W->n_trip * 7 + W->n_pair + 1)));
+    FCB_TRY(h->sw_blk2.ensure(sizeof(double) * 9 * ((size_t)W->n_trip * 3 + W->n_pair + 1)));
+    FCB_TRY(h->sw_atoms.ensure(sizeof(int4) * (size_t)(W->n_trip + 1) + sizeof(int2) * (size_t)(W->n_pair + 1)));
+    W->blk3 = h->sw_blk3.as<double>();
+    W->blk2 = h->sw_blk2.as<double>();
+    W->trip_atoms = h->sw_atoms.as<int4>();
+    W->pair_atoms = reinterpret_cast<int2*>(W->trip_atoms + W->n_trip + 1);
+    if (W->n_trip > 0) {
+        sw_triplet_kernel<<<(W->n_trip + TRIP_WARPS - 1) / TRIP_WARPS, 32 * TRIP_WARPS, 0, s>>>(
+            d_pos, N, W->nbr, W->nbr_r, W->cnt, W->trip_off, W->n_trip, P, W->blk3, W->blk2, W->trip_atoms);
+        FCB_CUDA(cudaGetLastError());
+    }
+    if (W->n_pair > 0) {
+        sw_pair_kernel<<<(W->n_pair + 127) / 128, 128, 0, s>>>(N, W->nbr, W->nbr_r, W->cnt, W->pair_off, W->n_pair, P,
+                                                               W->blk3 + (size_t)W->n_trip * 7 * 27,
+                                                               W->blk2 + (size_t)W->n_trip * 3 * 9, W->pair_atoms);
+        FCB_CUDA(cudaGetLastError());
+    }
+    return FCB_OK;
+}
+
+// Buckets of `np` placements by `kind` over N*N keys.
+static int sw_bucket(fcb200_context* h, Buf& offb, Buf& itemb, Buf& curb, const void* pl, int np, int kind, int N,
+                     cudaStream_t s, int** off, int** items) {
+    const int nb = N * N;
+    FCB_TRY(offb.ensure(sizeof(int) * (size_t)(nb + 1)));
+    FCB_TRY(curb.ensure(sizeof(int) * (size_t)(nb + 1)));
+    FCB_TRY(itemb.ensure(sizeof(int) * (size_t)(np + 1)));
+    int* cnt = curb.as<int>();
+    FCB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)nb, s));
+    const Place* P = static_cast<const Place*>(pl);
+    if (np > 0) bucket_count_kernel<<<(np + 255) / 256, 256, 0, s>>>(P, np, kind, N, cnt);
+    scan_kernel<<<1, 1024, 0, s>>>(cnt, nb, offb.as<int>());
+    FCB_CUDA(cudaMemcpyAsync(cnt, offb.p, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToDevice, s));
+    if (np > 0) bucket_fill_kernel<<<(np + 255) / 256, 256, 0, s>>>(P, np, kind, N, cnt, itemb.as<int>());
+    bucket_sort_kernel<<<(nb + 255) / 256, 256, 0, s>>>(P, kind, nb, offb.as<int>(), itemb.as<int>());
+    FCB_CUDA(cudaGetLastError());
+    (void)h;
+    *off = offb.as<int>();
+    *items = itemb.as<int>();
+    return FCB_OK;
+}
+
+static SwPot sw_pot(const double* cos0) {
+    SwPot P;
+    P.eps = 2.1683;
+    P.sigma = 2.0951;
+    P.a = 1.80;
+    P.lambda = 21.0;
+    P.gamma = 1.20;
+    P.A = 7.049556277;
+    P.B = 0.6022245584;
+    P.rc = P.a * P.sigma;
+    P.gs = P.sigma * P.gamma;
+    P.le = P.eps * P.lambda;
+    P.cos0_gen = cos0 ? cos0[0] : -0.333333333333;
+    P.cos0_iik = cos0 ? cos0[1] : -1.0 / 3.0;
+    return P;
+}
+
+double sw_potential_cutoff() { return sw_pot(nullptr).rc; }
+
+int sw_third_order_launch(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double r_cut,
+                          const double* cos0, double tol, const double* d_masses, const AssemblyOut& out,
+                          cudaStream_t s) {
+    const SwPot P = sw_pot(cos0);
+    SwWork W;
+    FCB_TRY(sw_prepare(h, d_pos, (int)N, d_box, r_cut, P, s, &W));
+    const int np = W.n_trip * 24 + W.n_pair * 6;
+    FCB_TRY(h->sw_place.ensure(sizeof(Place) * (size_t)(np + 1)));
+    Place* pl = h->sw_place.as<Place>();
+    if (W.n_trip + W.n_pair > 0)
+        sw_place3_kernel<<<(W.n_trip + W.n_pair + 127) / 128, 128, 0, s>>>(W.trip_atoms, W.n_trip, W.pair_atoms,
+                                                                             W.n_pair, (int)N, pl);
+    int *col_off, *col_items, *asr_off, *asr_items;
+    FCB_TRY(sw_bucket(h, h->sw_col_off, h->sw_col_items, h->sw_cursor, pl, np, 0, (int)N, s, &col_off, &col_items));
+    FCB_TRY(sw_bucket(h, h->sw_asr_off, h->sw_asr_items, h->sw_cursor, pl, np, 1, (int)N, s, &asr_off, &asr_items));
+    FCB_TRY(h->sw_asr.ensure(sizeof(double) * 27 * (size_t)N * N));
+    const int64_t na = (int64_t)N * N * 27;
+    sw_asr3_kernel<<<(unsigned)((na + 255) / 256), 256, 0, s>>>(pl, W.blk3, (int)(N * N), asr_off, asr_items,
+                                                                   h->sw_asr.as<double>());
+    SwDense g;
+    g.N = (int)N;
+    g.n = (int)(3 * N);
+    g.n_pad = out.n_pad ? out.n_pad : 3 * N;
+    g.tol = tol;
+    g.pl = pl;
+    g.blocks = W.blk3;
+    g.col_off = col_off;
+    g.col_items = col_items;
+    g.asr_off = asr_off;
+    g.S = h->sw_asr.as<double>();
+    g.masses = d_masses;
+    g.psi64 = out.psi64;
+    g.psi64_weighted = out.psi64_weighted;
+    g.psi32 = out.psi32;
+    g.split_hi = out.split_hi;
+    g.split_lo = out.split_lo;
+    g.split_kind = out.split_kind;
+    const int64_t cols = (int64_t)g.n * g.n;
+    int64_t blocks = (cols + 7) / 8;
+    if (blocks > (int64_t)h->sm_count * 8) blocks = (int64_t)h->sm_count * 8;
+    sw_dense_kernel<<<(unsigned)blocks, 256, 0, s>>>(g);
+    FCB_CUDA(cudaGetLastError());
+    return FCB_OK;
+}
+
+int sw_second_order_launch(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double r_cut,
+                           const double* cos0, double tol, const double* d_masses, double* d_ifc2, cudaStream_t s) {
+    const SwPot P = sw_pot(cos0);
+    SwWork W;
+    FCB_TRY(sw_prepare(h, d_pos, (int)N, d_box, r_cut, P, s, &W));
+    const int np = W.n_trip * 6 + W.n_pair * 2;
+    FCB_TRY(h->sw_place.ensure(sizeof(Place) * (size_t)(np + 1)));
+    Place* pl = h->sw_place.as<Place>();
+    if (W.n_trip + W.n_pair > 0)
+        sw_place2_kernel<<<(W.n_trip + W.n_pair + 127) / 128, 128, 0, s>>>(W.trip_atoms, W.n_trip, W.pair_atoms,
+                                                                             W.n_pair, (int)N, pl);
+    int *off, *items;
+    FCB_TRY(sw_bucket(h, h->sw_col_off, h->sw_col_items, h->sw_cursor, pl, np, 2, (int)N, s, &off, &items));
+    const int64_t nn = 9 * N * N;
+    sw_ifc2_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>((int)N, tol, pl, W.blk2, off, items, d_masses, d_ifc2);
+    FCB_CUDA(cudaGetLastError());
+    return FCB_OK;
+}
+
+}  // namespace fcb

@@ -49,6 +49,8 @@ SIGNATURES = {
     "fcb200_set_profiling": (_I, [_P, _I]),
     "fcb200_phase_times": (_I, [_P, ctypes.POINTER(_D), _I]),
     "fcb200_third_order_lj_noalloc": (_I, [_P, _I64, _P, _D, _D, _D, _D, _P, _P, _P, _I, _P]),
+    "fcb200_third_order_sw": (_I, [_P, _P, _I64, _P, _D, _D, _P, _P, _P, _P, _I, _P]),
+    "fcb200_second_order_sw": (_I, [_P, _P, _I64, _P, _D, _D, _P, _P, _P, _P]),
 }
 
 _lib = None
@@ -93,7 +95,7 @@ def check(status: int) -> None:
         return
     code, msg = last_error()
     if status == FCB_ERR_CUTOFF:
-        raise AssertionError("Cutoff larger than L/2")
+        raise AssertionError(msg if "SW" in msg else "Cutoff larger than L/2")
     if status == FCB_ERR_BLOCK:
         raise AssertionError("size(phi)[1] % block_size == 0")
     raise FCB200Error(status, msg)

@@ -119,6 +119,33 @@ int fcb200_second_order_lj(fcb200_handle h, const double* pos, int64_t n_atoms, 
                            const double* masses, double* ifc2_out, void* stream);
 
 /*
+ * Dense third-order IFCs of Stillinger-Weber silicon (LAMMPS Si.sw parameters,
+ * eV and Å), the AutoDiffCalculator path of the reference.  Replaces
+ *   third_order(sys, ::StillingerWeberSilicon, AutoDiffCalculator(tol, r_cut))
+ *     src/ifc.jl:20-35, src/autodiff/third_order_AD.jl:71-224, src/asr.jl:19-40
+ * with analytic derivatives instead of generated AD kernels.  cos0 = {cosθ₀
+ * of the blocks the reference takes from its generated kernels (written there
+ * as -0.333333333333), cosθ₀ of the iik block (built at run time from the exact
+ * -1/3)}; NULL selects exactly those values.  r_cut must not exceed the SW
+ * cutoff aσ (third_order_AD.jl:74), else FCB_ERR_CUTOFF.  Outputs as in
+ * fcb200_third_order_lj.  Synchronises the stream (it sizes its scratch from
+ * the neighbour count).
+ */
+int fcb200_third_order_sw(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                          double r_cut, double tol, const double* cos0, const double* masses,
+                          double* psi_out, float* psi32_mw_out, int flags, void* stream);
+
+/*
+ * Dense second-order IFCs of Stillinger-Weber silicon; with masses != NULL the
+ * dynamical matrix.  Replaces second_order(sys, ::StillingerWeberSilicon,
+ * AutoDiffCalculator) — src/ifc.jl:3-18, src/autodiff/second_order_AD.jl:40-110,
+ * src/asr.jl:3-17, src/dynmat.jl:5-33.  cos0 as above (only cos0[0] is used).
+ */
+int fcb200_second_order_sw(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                           double r_cut, double tol, const double* cos0, const double* masses,
+                           double* ifc2_out, void* stream);
+
+/*
  * Third-order modal coupling constants
  *   K3[a,b,c] = Σ_ijk Ψ[i,j,k] φ[i,n_lo+a] φ[j,m_lo+b] φ[k,l_lo+c]
  * for the mode windows [n_lo,n_hi) × [m_lo,m_hi) × [l_lo,l_hi), as three

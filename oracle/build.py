@@ -52,10 +52,12 @@ def build_reference_translation(reference_root: str | None = None, force: bool =
         return lib if os.path.exists(lib) else None
     os.makedirs(REF_OUT, exist_ok=True)
     c_path = os.path.join(REF_OUT, "sw_generated.c")
-    if force or not os.path.exists(c_path) or not os.path.exists(lib):
+    deps = [os.path.join(HERE, "sw_oracle.c"), os.path.join(HERE, "lj_oracle.c")]
+    if force or not os.path.exists(c_path):
         translate_all(gen_dir, c_path)
-        cmd = ["gcc", "-O1", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", c_path,
-               "-o", lib, "-lm"]
+    if force or _stale(lib, [c_path, *deps]):
+        cmd = ["gcc", "-O1", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+               "-DSW_BLOCKS_FROM_REFERENCE", *deps, c_path, "-o", lib, "-lm"]
         subprocess.run(cmd, check=True)
     return lib
 

@@ -50,13 +50,62 @@ def lib():
         L.oracle_lj_derivs.argtypes = [_D, _D, _D, _PD]
         L.oracle_set_num_threads.argtypes = [ctypes.c_int]
         L.oracle_num_threads.restype = ctypes.c_int
-        if hasattr(L, "oracle_third_order_sw"):
-            L.oracle_third_order_sw.argtypes = [_PD, _I64, _PD, _PD, _D, _D, _PD]
-            L.oracle_third_order_sw.restype = ctypes.c_int
-            L.oracle_second_order_sw.argtypes = [_PD, _I64, _PD, _PD, _D, _D, _PD]
-            L.oracle_second_order_sw.restype = ctypes.c_int
+        _sw_signatures(L)
         _lib = L
     return _lib
+
+
+def _sw_signatures(L):
+    L.oracle_third_order_sw.argtypes = [_PD, _I64, _PD, _PD, _D, _D, _PD]
+    L.oracle_third_order_sw.restype = ctypes.c_int
+    L.oracle_second_order_sw.argtypes = [_PD, _I64, _PD, _PD, _D, _D, _PD]
+    L.oracle_second_order_sw.restype = ctypes.c_int
+    L.oracle_sw_triplet_blocks.argtypes = [_PD, _PD, _PD]
+    L.oracle_sw_triplet_blocks2.argtypes = [_PD, _PD, _PD]
+    L.oracle_sw_pair_block3.argtypes = [_PD, _PD]
+    L.oracle_sw_pair_block2.argtypes = [_PD, _PD]
+    L.oracle_sw_rcut.restype = ctypes.c_double
+
+
+_ref = None
+
+
+def ref_lib():
+    """oracle/_ref/libswref.so: the same SW loop driven by the reference's own
+    generated derivative kernels (built only where the reference checkout is
+    present; None otherwise)."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libswref.so")
+        if not os.path.exists(path):
+            return None
+        L = ctypes.CDLL(path)
+        _sw_signatures(L)
+        _ref = L
+    return _ref
+
+
+COS0_GEN = -0.333333333333
+COS0_IIK = -1.0 / 3.0
+
+
+def sw_blocks(r9, cos0=(COS0_GEN, COS0_IIK), use_ref=False):
+    """The 7 third-derivative blocks (iij, ijj, iik, ikk, jjk, jkk, ijk) of one
+    SW triplet from 9 absolute coordinates; column-major 3×3×3 each."""
+    L = ref_lib() if use_ref else lib()
+    r9 = np.ascontiguousarray(r9, dtype=np.float64)
+    c = np.ascontiguousarray(cos0, dtype=np.float64)
+    out = np.zeros(7 * 27)
+    L.oracle_sw_triplet_blocks(_pd(r9), _pd(c), _pd(out))
+    return out.reshape(7, 27)
+
+
+def sw_pair_block(r3, use_ref=False):
+    L = ref_lib() if use_ref else lib()
+    r3 = np.ascontiguousarray(r3, dtype=np.float64)
+    out = np.zeros(27)
+    L.oracle_sw_pair_block3(_pd(r3), _pd(out))
+    return out
 
 
 def _pd(a):
@@ -107,9 +156,9 @@ def mass_weight_third_order(psi, masses):
     return psi
 
 
-def third_order_sw(pos, box, r_cut, tol, cos0_generated=-0.333333333333, cos0_iik=-1.0 / 3.0):
+def third_order_sw(pos, box, r_cut, tol, cos0_generated=-0.333333333333, cos0_iik=-1.0 / 3.0, use_ref=False):
     """third_order_AD.jl:71-170 + ifc.jl:20-35 for Stillinger-Weber silicon."""
-    L = lib()
+    L = ref_lib() if use_ref else lib()
     pos, N = _pos(pos)
     box = np.ascontiguousarray(box, dtype=np.float64)
     n = 3 * N
@@ -121,8 +170,9 @@ def third_order_sw(pos, box, r_cut, tol, cos0_generated=-0.333333333333, cos0_ii
     return psi.reshape((n, n, n), order="F")
 
 
-def second_order_sw(pos, box, r_cut, tol, cos0_generated=-0.333333333333):
-    L = lib()
+def second_order_sw(pos, box, r_cut, tol, cos0_generated=-0.333333333333, use_ref=False):
+    """second_order_AD.jl:40-110 + ifc.jl:3-18 for Stillinger-Weber silicon."""
+    L = ref_lib() if use_ref else lib()
     pos, N = _pos(pos)
     box = np.ascontiguousarray(box, dtype=np.float64)
     n = 3 * N
