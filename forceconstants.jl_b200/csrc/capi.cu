@@ -256,7 +256,8 @@ int fcb200_trim(fcb200_handle h) {
                    &h->u2_hi, &h->u2_lo, &h->u1_f32, &h->u2_f32, &h->psi_f32, &h->k3_stage[0],
                    &h->k3_stage[1], &h->ifc2, &h->sw_ints, &h->sw_nbr_r, &h->sw_pair_off, &h->sw_blk3,
                    &h->sw_blk2, &h->sw_atoms, &h->sw_place, &h->sw_col_off, &h->sw_col_items, &h->sw_cursor,
-                   &h->sw_asr_off, &h->sw_asr_items, &h->sw_asr};
+                   &h->sw_asr_off, &h->sw_asr_items, &h->sw_asr, &h->adj_phiT, &h->adj_w_hi, &h->adj_w_lo,
+                   &h->adj_pairs, &h->adj_G, &h->adj_scal, &h->adj_w32, &h->adj_dpos};
     for (Buf* b : bufs) b->release();
     return FCB_OK;
 }
@@ -542,32 +543,21 @@ int fcb200_mcc3_blocked(fcb200_handle h, const float* psi, const float* phi, int
     return FCB_OK;
 }
 
-int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t N, const double* box, double sigma, double eps,
-                       double r_cut, double tol, const double* masses, const float* phi, int64_t mode_lo,
-                       int64_t mode_hi, int precision, double* psi_out, float* k3_out, void* stream) {
-    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
-    FCB_TRY(validate_lj(pos, N, box, r_cut, masses, true));
-    if (!phi || !k3_out) return set_error(FCB_ERR_ARG, "phi and k3_out must not be NULL");
+}  // extern "C"
+
+namespace fcb {
+namespace {
+// Snapshot driver shared by the LJ and SW entry points: `assemble` writes Ψ
+// (optional FP64) and the operand of the chosen precision in one pass, then the
+// three mode products run.
+template <class Assemble>
+int snapshot_run(fcb200_context* h, int64_t N, const float* phi, int64_t mode_lo, int64_t mode_hi, int precision,
+                 double* psi_out, float* k3_out, cudaStream_t s, bool host_inputs, Assemble assemble) {
     const int64_t n = 3 * N;
-    if (!mcc3_ranges_ok(n, mode_lo, mode_hi)) return set_error(FCB_ERR_ARG, "mode window outside [0, n)");
-    FCB_TRY(check_precision(precision));
-    double bh[3];
-    FCB_TRY(box_to_host(box, bh));
-    FCB_TRY(check_cutoff(bh));
-    for (int d = 0; d < 3; ++d)
-        if (!(r_cut < bh[d])) return set_error(FCB_ERR_CUTOFF, "Cutoff larger than L/2 (r_cut must be < box length)");
-    cudaSetDevice(h->device);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    double *d_pos, *d_box, *d_m;
     float* d_phi;
-    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
-    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
-    FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
     FCB_TRY(device_view(h->phi_f32, phi, (size_t)(n * n), true, s, &d_phi));
     for (bool& m : h->marked) m = false;
     phase_mark(h, s, 0);
-    FCB_TRY(lj_pair_tables(h, d_pos, N, d_box, sigma, eps, r_cut, s));
-    phase_mark(h, s, 1);
     const bool host64 = psi_out && !is_device_ptr(psi_out);
     if (host64) FCB_TRY(h->psi_stage.ensure(sizeof(double) * n * n * n));
     AssemblyOut out;
@@ -589,14 +579,14 @@ int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t N, const doub
         op.hi = out.split_hi;
         op.lo = out.split_lo;
     }
-    FCB_TRY(ifc3_dense_write(h, N, tol, d_m, out, s));
+    FCB_TRY(assemble(out));  // marks 1 (after the pair/triplet tables) itself
     phase_mark(h, s, 2);
     if (precision == FCB_MCC3_FP32) phase_mark(h, s, 3);  // no φ split phase
     const int64_t M = mode_hi - mode_lo;
     float* d_k3;
     FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)(M * M * M), false, s, &d_k3));
     FCB_TRY(run_mcc3(h, precision, op, d_phi, n, mode_lo, mode_hi, mode_lo, mode_hi, mode_lo, mode_hi, d_k3, s));
-    bool host = false;
+    bool host = host_inputs || d_phi != phi;
     if (host64) {
         FCB_CUDA(cudaMemcpyAsync(psi_out, out.psi64, sizeof(double) * n * n * n, cudaMemcpyDeviceToHost, s));
         host = true;
@@ -605,8 +595,103 @@ int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t N, const doub
         FCB_CUDA(cudaMemcpyAsync(k3_out, d_k3, sizeof(float) * M * M * M, cudaMemcpyDeviceToHost, s));
         host = true;
     }
-    if (host || d_pos != pos || d_phi != phi) return check_status(h, s);
+    if (host) return check_status(h, s);
     return FCB_OK;
+}
+}  // namespace
+}  // namespace fcb
+
+extern "C" {
+
+int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t N, const double* box, double sigma, double eps,
+                       double r_cut, double tol, const double* masses, const float* phi, int64_t mode_lo,
+                       int64_t mode_hi, int precision, double* psi_out, float* k3_out, void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    FCB_TRY(validate_lj(pos, N, box, r_cut, masses, true));
+    if (!phi || !k3_out) return set_error(FCB_ERR_ARG, "phi and k3_out must not be NULL");
+    const int64_t n = 3 * N;
+    if (!mcc3_ranges_ok(n, mode_lo, mode_hi)) return set_error(FCB_ERR_ARG, "mode window outside [0, n)");
+    FCB_TRY(check_precision(precision));
+    double bh[3];
+    FCB_TRY(box_to_host(box, bh));
+    FCB_TRY(check_cutoff(bh));
+    for (int d = 0; d < 3; ++d)
+        if (!(r_cut < bh[d])) return set_error(FCB_ERR_CUTOFF, "Cutoff larger than L/2 (r_cut must be < box length)");
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double *d_pos, *d_box, *d_m;
+    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
+    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
+    FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
+    return snapshot_run(h, N, phi, mode_lo, mode_hi, precision, psi_out, k3_out, s, d_pos != pos,
+                        [&](const AssemblyOut& out) {
+                            FCB_TRY(lj_pair_tables(h, d_pos, N, d_box, sigma, eps, r_cut, s));
+                            phase_mark(h, s, 1);
+                            return ifc3_dense_write(h, N, tol, d_m, out, s);
+                        });
+}
+
+int fcb200_mcc3_adjoint_lj(fcb200_handle h, const double* pos, int64_t N, const double* box, double sigma,
+                           double eps, double r_cut, const double* masses, const float* phi, int64_t n_modes,
+                           const float* W, int precision, double* dpos, double* dsigma, double* deps, double* L_out,
+                           void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    FCB_TRY(validate_lj(pos, N, box, r_cut, masses, true));
+    if (!phi || !W || !dpos) return set_error(FCB_ERR_ARG, "phi, W and dpos must not be NULL");
+    const int64_t n = 3 * N;
+    if (n_modes < 1 || n_modes > n) return set_error(FCB_ERR_ARG, "n_modes must be in [1, 3*n_atoms]");
+    FCB_TRY(check_precision(precision));
+    double bh[3];
+    FCB_TRY(box_to_host(box, bh));
+    FCB_TRY(check_cutoff(bh));
+    for (int d = 0; d < 3; ++d)
+        if (!(r_cut < bh[d])) return set_error(FCB_ERR_CUTOFF, "Cutoff larger than L/2 (r_cut must be < box length)");
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double *d_pos, *d_box, *d_m, *d_dpos;
+    float *d_phi, *d_W;
+    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
+    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
+    FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
+    FCB_TRY(device_view(h->phi_f32, phi, (size_t)(n * n), true, s, &d_phi));
+    FCB_TRY(device_view(h->adj_w32, W, (size_t)(n_modes * n_modes * n_modes), true, s, &d_W));
+    FCB_TRY(device_view(h->adj_dpos, (const double*)dpos, (size_t)(3 * N), false, s, &d_dpos));
+    FCB_TRY(h->adj_G.ensure(sizeof(float) * (size_t)(n * n * n)));
+    FCB_TRY(h->adj_scal.ensure(sizeof(double) * 4));
+    FCB_TRY(adjoint_g(h, precision, d_W, n_modes, d_phi, n, h->adj_G.as<float>(), s));
+    FCB_TRY(lj_adjoint_pairs(h, d_pos, N, d_box, sigma, eps, r_cut, d_m, h->adj_G.as<float>(), d_dpos,
+                             h->adj_scal.as<double>(), s));
+    double sc[3];
+    FCB_CUDA(cudaMemcpyAsync(sc, h->adj_scal.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (d_dpos != dpos) FCB_CUDA(cudaMemcpyAsync(dpos, d_dpos, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s));
+    FCB_TRY(check_status(h, s));
+    if (dsigma) *dsigma = sc[0];
+    if (deps) *deps = sc[1];
+    if (L_out) *L_out = sc[2];
+    return FCB_OK;
+}
+
+int fcb200_snapshot_sw(fcb200_handle h, const double* pos, int64_t N, const double* box, double r_cut, double tol,
+                       const double* cos0, const double* masses, const float* phi, int64_t mode_lo, int64_t mode_hi,
+                       int precision, double* psi_out, float* k3_out, void* stream) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    FCB_TRY(validate_sw(pos, N, box, r_cut));
+    if (!masses) return set_error(FCB_ERR_ARG, "masses are required for mass weighting");
+    if (!phi || !k3_out) return set_error(FCB_ERR_ARG, "phi and k3_out must not be NULL");
+    const int64_t n = 3 * N;
+    if (!mcc3_ranges_ok(n, mode_lo, mode_hi)) return set_error(FCB_ERR_ARG, "mode window outside [0, n)");
+    FCB_TRY(check_precision(precision));
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double *d_pos, *d_box, *d_m;
+    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
+    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
+    FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
+    return snapshot_run(h, N, phi, mode_lo, mode_hi, precision, psi_out, k3_out, s, d_pos != pos,
+                        [&](const AssemblyOut& out) {
+                            phase_mark(h, s, 1);
+                            return sw_third_order_launch(h, d_pos, N, d_box, r_cut, cos0, tol, d_m, out, s);
+                        });
 }
 
 }  // extern "C"

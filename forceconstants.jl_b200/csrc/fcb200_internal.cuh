@@ -76,6 +76,8 @@ struct fcb200_context {
     // Stillinger-Weber scratch (neighbours, blocks, placements, buckets, ASR rows)
     fcb::Buf sw_ints, sw_nbr_r, sw_pair_off, sw_blk3, sw_blk2, sw_atoms, sw_place;
     fcb::Buf sw_col_off, sw_col_items, sw_cursor, sw_asr_off, sw_asr_items, sw_asr;
+    // adjoint scratch
+    fcb::Buf adj_phiT, adj_w_hi, adj_w_lo, adj_pairs, adj_G, adj_scal, adj_w32, adj_dpos;
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // Optional per-phase timing of fcb200_snapshot_lj (events on the caller's stream).
@@ -131,6 +133,13 @@ int sw_third_order_launch(fcb200_context* h, const double* d_pos, int64_t N, con
                           cudaStream_t s);
 int sw_second_order_launch(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double r_cut,
                            const double* cos0, double tol, const double* d_masses, double* d_ifc2, cudaStream_t s);
+
+// Adjoint (adjoint.cu)
+int adjoint_g(fcb200_context* h, int precision, const float* d_W, int64_t M, const float* d_phi, int64_t n,
+              float* d_G, cudaStream_t s);
+int lj_adjoint_pairs(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
+                     double eps, double r_cut, const double* d_masses, const float* d_G, double* d_dpos,
+                     double* d_scal, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // mcc3 (mcc3.cu, mode_product_simt.cu, mode_product_tc.cu)

@@ -51,6 +51,9 @@ SIGNATURES = {
     "fcb200_third_order_lj_noalloc": (_I, [_P, _I64, _P, _D, _D, _D, _D, _P, _P, _P, _I, _P]),
     "fcb200_third_order_sw": (_I, [_P, _P, _I64, _P, _D, _D, _P, _P, _P, _P, _I, _P]),
     "fcb200_second_order_sw": (_I, [_P, _P, _I64, _P, _D, _D, _P, _P, _P, _P]),
+    "fcb200_snapshot_sw": (_I, [_P, _P, _I64, _P, _D, _D, _P, _P, _P, _I64, _I64, _I, _P, _P, _P]),
+    "fcb200_mcc3_adjoint_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _P, _P, _I64, _P, _I, _P,
+                                    ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D), _P]),
 }
 
 _lib = None

@@ -77,14 +77,23 @@ def mcc3_window(psi, phi, n_range, m_range, l_range, precision: str = "fp32"):
 def snapshot_lj(sys, pot, calc, phi, precision: str = "bf16x3", modes=None, psi_out=None, k3_out=None,
                 stream: int = 0):
     """Fused third_order → mass_weight_third_order! → Float32 → mcc3 for one
-    LJ snapshot, without the host round trip.  Buffers may be host or device;
-    returns (psi_out, k3_out)."""
+    snapshot (LJ, or Stillinger-Weber when ``pot`` is a
+    StillingerWeberSilicon), without the host round trip.  Buffers may be host
+    or device; returns (psi_out, k3_out)."""
+    from .types import StillingerWeberSilicon
     n = 3 * sys.n_atoms
     lo, hi = (0, n) if modes is None else (int(modes[0]), int(modes[1]))
     M = hi - lo
     if k3_out is None:
         k3_out = julia_empty((M, M, M), np.float32, "cuda" if is_torch(phi) and phi.is_cuda else "cpu")
     dev = device_index(phi) if is_torch(phi) else 0
+    if isinstance(pot, StillingerWeberSilicon):
+        c0 = np.array([-0.333333333333, float(pot.cos0)], dtype=np.float64)
+        _lib.check(_lib.lib().fcb200_snapshot_sw(
+            _lib.handle(dev), ptr(sys.positions), sys.n_atoms, ptr(sys.box_sizes), float(calc.r_cut),
+            float(calc.tol), ptr(c0), ptr(sys.masses), ptr(phi), lo, hi, _lib.PRECISIONS[precision],
+            ptr(psi_out), ptr(k3_out), stream or stream_ptr(k3_out)))
+        return psi_out, k3_out
     _lib.check(_lib.lib().fcb200_snapshot_lj(
         _lib.handle(dev), ptr(sys.positions), sys.n_atoms, ptr(sys.box_sizes), float(pot.sigma), float(pot.eps),
         float(calc.r_cut), float(calc.tol), ptr(sys.masses), ptr(phi), lo, hi, _lib.PRECISIONS[precision],

@@ -188,6 +188,34 @@ int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t n_atoms, cons
                        double* psi_out, float* k3_out, void* stream);
 
 /*
+ * One Stillinger-Weber snapshot end to end: SW IFC3 assembly (as
+ * fcb200_third_order_sw) with the fused mass-weighted operand, then mcc3 over
+ * modes [mode_lo, mode_hi) on every axis.  Same composition as
+ * fcb200_snapshot_lj for the reference's AutoDiffCalculator SW path.
+ */
+int fcb200_snapshot_sw(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                       double r_cut, double tol, const double* cos0, const double* masses,
+                       const float* phi, int64_t mode_lo, int64_t mode_hi, int precision,
+                       double* psi_out, float* k3_out, void* stream);
+
+/*
+ * Adjoint of an LJ snapshot (no counterpart in the reference, which has no
+ * gradients): for L = Σ_abc W[a,b,c] K3[a,b,c] with K3 over modes [0,n_modes)
+ * on every axis (φ frozen), the gradients ∂L/∂positions (dpos, 3*n_atoms
+ * doubles), ∂L/∂σ and ∂L/∂ε, and L itself.  G = W ×₁φᵀ ×₂φᵀ ×₃φᵀ is formed by
+ * the transposed mode products (precision as for mcc3), then every pair inside
+ * the cutoff contracts its recomputed ϕ₃ blocks (third_order_analytical.jl:216-224),
+ * their fourth derivatives ϕ₄ (fourth_order_analytical.jl:184-198) and
+ * σ-derivatives with G; Ψ and the fourth-order tensor are never stored.  The
+ * tolerance cutoff of Ψ is not differentiated.  W is n_modes³ floats,
+ * column-major.  Synchronises the stream.
+ */
+int fcb200_mcc3_adjoint_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                           double sigma, double eps, double r_cut, const double* masses,
+                           const float* phi, int64_t n_modes, const float* W, int precision,
+                           double* dpos, double* dsigma, double* deps, double* L_out, void* stream);
+
+/*
  * Device-side phase timing (no counterpart in the reference, which has no
  * instrumentation).  With profiling enabled, fcb200_snapshot_lj records CUDA
  * events on the caller's stream between its phases; fcb200_phase_times then

@@ -49,6 +49,7 @@ def lib():
         L.oracle_cast_f32.argtypes = [_PD, _PF, _I64]
         L.oracle_lj_derivs.argtypes = [_D, _D, _D, _PD]
         L.oracle_set_num_threads.argtypes = [ctypes.c_int]
+        L.oracle_nearest_mirror.argtypes = [_PD, _PD]
         L.oracle_num_threads.restype = ctypes.c_int
         _sw_signatures(L)
         _lib = L
@@ -237,3 +238,84 @@ def lj_derivs(sigma, eps, r):
     d = np.zeros(4)
     lib().oracle_lj_derivs(sigma, eps, r, _pd(d))
     return d
+
+
+# ------------------------------------------------------------------ adjoint
+def mcc3_loss_lj(pos, box, sigma, eps, r_cut, masses, phi, W, tol=1e-12):
+    """L = Σ W·K3 in FP64 along the reference path (third_order → mass weight
+    → mcc3 over modes [0, M)); used for central finite differences."""
+    psi = third_order_lj(pos, box, sigma, eps, r_cut, tol)
+    mw = mass_weight_third_order(psi, masses)
+    M = W.shape[0]
+    return float(np.sum(W * mcc3(mw, phi, modes=(0, M))))
+
+
+def _lj_rad(r, sg, ep):
+    """Φ′..Φ⁗ (LennardJones.jl:38-56) and the σ-derivatives of Φ′..Φ‴."""
+    d1 = -ep * (48 * sg ** 12 / r ** 13 - 24 * sg ** 6 / r ** 7)
+    d2 = 4 * ep * (156 * sg ** 12 / r ** 14 - 42 * sg ** 6 / r ** 8)
+    d3 = -4 * ep * (2184 * sg ** 12 / r ** 15 - 336 * sg ** 6 / r ** 9)
+    d4 = 4 * ep * (32760 * sg ** 12 / r ** 16 - 3024 * sg ** 6 / r ** 10)
+    s1 = -ep * (576 * sg ** 11 / r ** 13 - 144 * sg ** 5 / r ** 7)
+    s2 = 4 * ep * (1872 * sg ** 11 / r ** 14 - 252 * sg ** 5 / r ** 8)
+    s3 = -4 * ep * (26208 * sg ** 11 / r ** 15 - 2016 * sg ** 5 / r ** 9)
+    return d1, d2, d3, d4, s1, s2, s3
+
+
+def _phi3_t(f1, f2, f3, nh, r):
+    """ϕ₃ tensor (third_order_analytical.jl:216-224) from radial derivatives."""
+    A = f3 - 3 * f2 / r + 3 * f1 / r ** 2
+    B = (f2 - f1 / r) / r
+    I = np.eye(3)
+    return (np.einsum('a,b,c->abc', nh, nh, nh) * A +
+            B * (np.einsum('bc,a->abc', I, nh) + np.einsum('ca,b->abc', I, nh) + np.einsum('ab,c->abc', I, nh)))
+
+
+def _phi4_t(d1, d2, d3, d4, nh, r):
+    """ϕ₄ tensor (fourth_order_analytical.jl:184-198)."""
+    I = np.eye(3)
+    E4 = d4 - 6 * d3 / r + 15 * d2 / r ** 2 - 15 * d1 / r ** 3
+    E3 = (d3 - 3 * d2 / r + 3 * d1 / r ** 2) / r
+    E2 = (d2 - d1 / r) / r ** 2
+    nn = np.einsum('a,b->ab', nh, nh)
+    v = sum(np.einsum(s, nn, I) for s in ['ab,cd->abcd', 'ac,bd->abcd', 'ad,bc->abcd',
+                                             'bc,ad->abcd', 'bd,ac->abcd', 'cd,ab->abcd'])
+    dd = np.einsum('ab,cd->abcd', I, I) + np.einsum('ac,bd->abcd', I, I) + np.einsum('ad,bc->abcd', I, I)
+    return np.einsum('a,b,c,d->abcd', nh, nh, nh, nh) * E4 + v * E3 + dd * E2
+
+
+def lj_adjoint(pos, box, sigma, eps, r_cut, masses, phi, W):
+    """FP64 gradient of L = Σ W·K3 by the pair form of the chain rule:
+    G = W ×₁φᵀ ×₂φᵀ ×₃φᵀ, C_AB = G'[AAA] − G'[AAB] − G'[ABA] − G'[BAA],
+    ∂L/∂r_A = Σ_B ϕ₄(d_AB)·C_AB − Σ_B ϕ₄(d_BA)·C_BA, ∂L/∂ε = L/ε,
+    ∂L/∂σ = Σ (∂ϕ₃/∂σ)·C.  Returns (dpos (N,3), dsigma, deps, L)."""
+    pos = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+    N = pos.shape[0]
+    M = W.shape[0]
+    ph = np.asarray(phi, dtype=np.float64)[:, :M]
+    G = np.einsum('abc,ia,jb,kc->ijk', np.asarray(W, dtype=np.float64), ph, ph, ph)
+    m = np.repeat(np.asarray(masses, dtype=np.float64), 3)
+    Gp = G / np.sqrt(m[:, None, None] * m[None, :, None] * m[None, None, :])
+    grad = np.zeros((N, 3))
+    dsg = 0.0
+    L = 0.0
+    for A in range(N):
+        for B in range(N):
+            if A == B:
+                continue
+            r = np.array(pos[A] - pos[B])
+            oracle_r = r.copy()
+            lib().oracle_nearest_mirror(_pd(oracle_r), _pd(np.ascontiguousarray(box, dtype=np.float64)))
+            rn = np.sqrt(oracle_r @ oracle_r)
+            if not rn < r_cut:
+                continue
+            nh = oracle_r / rn
+            d1, d2, d3, d4, s1, s2, s3 = _lj_rad(rn, sigma, eps)
+            a, b = slice(3 * A, 3 * A + 3), slice(3 * B, 3 * B + 3)
+            C = Gp[a, a, a] - Gp[a, a, b] - Gp[a, b, a] - Gp[b, a, a]
+            L += np.sum(_phi3_t(d1, d2, d3, nh, rn) * C)
+            dsg += np.sum(_phi3_t(s1, s2, s3, nh, rn) * C)
+            v = np.einsum('abcd,abc->d', _phi4_t(d1, d2, d3, d4, nh, rn), C)
+            grad[A] += v
+            grad[B] -= v
+    return grad, dsg, L / eps, L
