@@ -266,6 +266,7 @@ int fcb200_destroy(fcb200_handle h) {
     if (!h) return FCB_OK;
     cudaSetDevice(h->device);
     fcb200_trim(h);
+    if (h->owns_tune) delete h->tune;
     if (h->d_status) cudaFree(h->d_status);
     if (h->aux_stream) cudaStreamDestroy(h->aux_stream);
     for (auto& e : h->pev)
@@ -599,6 +600,19 @@ int snapshot_run(fcb200_context* h, int64_t N, const float* phi, int64_t mode_lo
     return FCB_OK;
 }
 }  // namespace
+
+// Device-pointer-only LJ snapshot without validation or host synchronisation
+// (inputs validated when they were added to a batch); safe inside stream capture.
+int snapshot_lj_device(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
+                       double eps, double r_cut, double tol, const double* d_m, const float* d_phi, int64_t mode_lo,
+                       int64_t mode_hi, int precision, float* d_k3, cudaStream_t s) {
+    return snapshot_run(h, N, d_phi, mode_lo, mode_hi, precision, nullptr, d_k3, s, false,
+                        [&](const AssemblyOut& out) {
+                            FCB_TRY(lj_pair_tables(h, d_pos, N, d_box, sigma, eps, r_cut, s));
+                            phase_mark(h, s, 1);
+                            return ifc3_dense_write(h, N, tol, d_m, out, s);
+                        });
+}
 }  // namespace fcb
 
 extern "C" {

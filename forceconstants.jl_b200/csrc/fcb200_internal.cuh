@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <unordered_map>
 
 #include "../../include/fcb200.h"
 
@@ -78,6 +79,10 @@ struct fcb200_context {
     fcb::Buf sw_col_off, sw_col_items, sw_cursor, sw_asr_off, sw_asr_items, sw_asr;
     // adjoint scratch
     fcb::Buf adj_phiT, adj_w_hi, adj_w_lo, adj_pairs, adj_G, adj_scal, adj_w32, adj_dpos;
+    // Autotuned mode-tile counts per mode-product shape (shared by a handle and
+    // its batch lanes; owned by the top-level handle).
+    std::unordered_map<uint64_t, int>* tune = nullptr;
+    bool owns_tune = false;
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // Optional per-phase timing of fcb200_snapshot_lj (events on the caller's stream).
@@ -90,6 +95,11 @@ struct fcb200_context {
 namespace fcb {
 
 bool is_device_ptr(const void* p);
+
+// Key of a mode-product shape in the autotune table.
+inline uint64_t tune_key(int kind, int64_t R, int64_t K, int64_t M) {
+    return ((uint64_t)kind << 62) ^ ((uint64_t)R << 24) ^ ((uint64_t)K << 12) ^ (uint64_t)M;
+}
 
 // Records phase mark i on stream s when profiling is enabled.
 inline void phase_mark(fcb200_context* h, cudaStream_t s, int i) {
@@ -133,6 +143,11 @@ int sw_third_order_launch(fcb200_context* h, const double* d_pos, int64_t N, con
                           cudaStream_t s);
 int sw_second_order_launch(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double r_cut,
                            const double* cos0, double tol, const double* d_masses, double* d_ifc2, cudaStream_t s);
+
+// Device-only snapshot (capi.cu), used by the batch engine (batch.cu).
+int snapshot_lj_device(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
+                       double eps, double r_cut, double tol, const double* d_m, const float* d_phi, int64_t mode_lo,
+                       int64_t mode_hi, int precision, float* d_k3, cudaStream_t s);
 
 // Adjoint (adjoint.cu)
 int adjoint_g(fcb200_context* h, int precision, const float* d_W, int64_t M, const float* d_phi, int64_t n,

@@ -462,6 +462,10 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
     p.F_pad = mp.F_pad;
     p.ldd = mp.ldd;
     p.n_tiles = (int)((mp.M + BN_MAX - 1) / BN_MAX);
+    if (h->tune) {  // autotuned mode-tile count for this shape, if any
+        auto it = h->tune->find(tune_key(kind, mp.R, mp.K, mp.M));
+        if (it != h->tune->end() && it->second >= p.n_tiles && it->second <= mp.M) p.n_tiles = it->second;
+    }
     const int64_t per = (mp.M + p.n_tiles - 1) / p.n_tiles;
     p.bn = (int)(((per + 15) / 16) * 16);
     p.m_tiles = (int)((mp.R + BM - 1) / BM);

@@ -52,6 +52,14 @@ SIGNATURES = {
     "fcb200_third_order_sw": (_I, [_P, _P, _I64, _P, _D, _D, _P, _P, _P, _P, _I, _P]),
     "fcb200_second_order_sw": (_I, [_P, _P, _I64, _P, _D, _D, _P, _P, _P, _P]),
     "fcb200_snapshot_sw": (_I, [_P, _P, _I64, _P, _D, _D, _P, _P, _P, _I64, _I64, _I, _P, _P, _P]),
+    "fcb200_autotune_mcc3": (_I, [_P, _I64, _I, ctypes.c_char_p, _P]),
+    "fcb200_batch_create": (_I, [_P, _I, ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "fcb200_batch_add_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _D, _P, _P, _P]),
+    "fcb200_batch_set_positions": (_I, [_P, _I64, _P, _P]),
+    "fcb200_batch_run": (_I, [_P, _P]),
+    "fcb200_batch_info": (_I, [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64),
+                               ctypes.POINTER(ctypes.c_size_t)]),
+    "fcb200_batch_destroy": (_I, [_P]),
     "fcb200_mcc3_adjoint_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _P, _P, _I64, _P, _I, _P,
                                     ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D), _P]),
 }

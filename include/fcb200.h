@@ -216,6 +216,37 @@ int fcb200_mcc3_adjoint_lj(fcb200_handle h, const double* pos, int64_t n_atoms, 
                            double* dpos, double* dsigma, double* deps, double* L_out, void* stream);
 
 /*
+ * Mode-product tile autotuner (no counterpart in the reference).  Times the
+ * candidate mode-tile counts of the tensor-core mode product for a full-mode
+ * mcc3 of side n (BF16×3 / TF32×3) and keeps the fastest in the handle; with
+ * cache_path != NULL the table is read from and written to that JSON file.
+ * Later mcc3, snapshot and batch calls of the handle use it.
+ */
+int fcb200_autotune_mcc3(fcb200_handle h, int64_t n, int precision, const char* cache_path, void* stream);
+
+/*
+ * Batches of LJ snapshots (no counterpart in the reference, which runs one
+ * snapshot at a time through third_order → mass_weight_third_order! → mcc3,
+ * README.md:69-76).  A batch keeps device copies of each snapshot's positions,
+ * box, masses and φ; fcb200_batch_run executes all of them: snapshots are
+ * admitted into up to 4 parallel lanes by HBM footprint (hbm_budget_bytes of
+ * scratch; 0 = 80 % of free memory), the first run executes eagerly and sizes
+ * every lane's scratch, and every later run replays the whole batch as ONE
+ * CUDA-graph launch on `stream`.  Ψ is kept only as the mass-weighted operand
+ * of the mode products.  k3_out must be device memory ((3N)³ floats).
+ */
+typedef struct fcb200_batch* fcb200_batch_t;
+int fcb200_batch_create(fcb200_handle h, int precision, size_t hbm_budget_bytes, fcb200_batch_t* out);
+int fcb200_batch_add_lj(fcb200_batch_t b, const double* pos, int64_t n_atoms, const double* box,
+                        double sigma, double eps, double r_cut, double tol, const double* masses,
+                        const float* phi, float* k3_out);
+int fcb200_batch_set_positions(fcb200_batch_t b, int64_t index, const double* pos, void* stream);
+int fcb200_batch_run(fcb200_batch_t b, void* stream);
+int fcb200_batch_info(fcb200_batch_t b, int64_t* n_snapshots, int64_t* lanes, int64_t* graph_nodes,
+                      size_t* scratch_bytes);
+int fcb200_batch_destroy(fcb200_batch_t b);
+
+/*
  * Device-side phase timing (no counterpart in the reference, which has no
  * instrumentation).  With profiling enabled, fcb200_snapshot_lj records CUDA
  * events on the caller's stream between its phases; fcb200_phase_times then

@@ -1,0 +1,81 @@
+"""Batched snapshots (fcb200_batch_*): every K3 of an eager run and of the
+CUDA-graph replays equals the single-snapshot path bit for bit (same kernels,
+same tiles), also after positions change between replays."""
+import numpy as np
+import pytest
+
+from conftest import AR, fcc_system
+
+pytestmark = pytest.mark.gpu
+
+
+def _phi(oracle, s):
+    ifc2 = oracle.second_order_lj(s.positions, s.box_sizes, AR["sigma"], AR["eps"], AR["r_cut"], 1e-12)
+    _, phi = oracle.get_modes(oracle.dynamical_matrix(ifc2, s.masses))
+    return np.asfortranarray(phi.astype(np.float32))
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "fp32"])
+def test_batch_matches_single_snapshots(fcb, oracle, cuda_device, precision):
+    import torch
+    from fcb200.batch import SnapshotBatch
+    pot = fcb.LJ(AR["sigma"], AR["eps"], AR["r_cut"])
+    calc = fcb.AnalyticalCalculator(1e-12, AR["r_cut"])
+    cells = [(2, 2, 2), (3, 3, 3), (2, 2, 2), (3, 3, 2), (2, 2, 3)]
+    systems = [fcc_system(c, 0.03 + 0.01 * i, 100 + i) for i, c in enumerate(cells)]
+    phis = [_phi(oracle, s) for s in systems]
+    b = SnapshotBatch(precision)
+    outs = [b.add(s, pot, calc, p) for s, p in zip(systems, phis)]
+
+    def single(s, p):
+        _, k = fcb.snapshot_lj(s, pot, calc, torch.from_numpy(p).cuda(), precision=precision)
+        torch.cuda.synchronize()
+        return k.cpu().numpy()
+
+    ref = [single(s, p) for s, p in zip(systems, phis)]
+    b.run()                 # eager
+    torch.cuda.synchronize()
+    for o, r in zip(outs, ref):
+        assert np.array_equal(o.cpu().numpy(), r)
+    for o in outs:
+        o.zero_()
+    b.run()                 # captured and replayed as one graph
+    b.run()
+    torch.cuda.synchronize()
+    info = b.info()
+    per_snapshot = 6 if precision == "fp32" else 7      # pair, self, dense, [phi split], 3 mode products
+    assert info["snapshots"] == len(systems) and info["lanes"] >= 1
+    assert info["graph_nodes"] >= per_snapshot * len(systems)
+    for o, r in zip(outs, ref):
+        assert np.array_equal(o.cpu().numpy(), r)
+    # new positions for snapshot 1, same graph
+    moved = fcb.displaced(systems[1], 0.02, 7)
+    b.set_positions(1, moved.positions)
+    b.run()
+    torch.cuda.synchronize()
+    assert np.array_equal(outs[1].cpu().numpy(), single(moved, phis[1]))
+    b.close()
+
+
+def test_batch_admission_refuses_oversize(fcb, cuda_device):
+    from fcb200 import _lib
+    from fcb200.batch import SnapshotBatch
+    s = fcc_system((2, 2, 2), 0.03, 1)
+    pot = fcb.LJ(AR["sigma"], AR["eps"], AR["r_cut"])
+    calc = fcb.AnalyticalCalculator(1e-12, AR["r_cut"])
+    b = SnapshotBatch("bf16x3", hbm_budget_bytes=1 << 20)   # 1 MiB of scratch: too small
+    b.add(s, pot, calc, np.eye(96, dtype=np.float32))
+    with pytest.raises(_lib.FCB200Error) as e:
+        b.run()
+    assert e.value.code == _lib.FCB_ERR_OOM
+    b.close()
+
+
+def test_autotune_cache_roundtrip(fcb, cuda_device, tmp_path):
+    from fcb200.batch import autotune_mcc3
+    path = str(tmp_path / "tune.json")
+    autotune_mcc3(96, "bf16x3", path)
+    text = open(path).read()
+    assert "mode_tiles" in text
+    autotune_mcc3(96, "bf16x3", path)     # cached: no retune, file stays valid
+    assert "mode_tiles" in open(path).read()
