@@ -307,25 +307,19 @@ def main():
         global CELLS
         CELLS = tuple(int(c) for c in args.cells.split(","))
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from fcb200 import replicas
+    rank, world, local = replicas.env_rank()
     import torch
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+    if args.impl == "reference":
+        # rank 0 alone runs the reference path; other ranks exit without work
+        # and without joining any collective.
+        if rank == 0:
+            run_reference(args, rank, world)
+        return
+    pg = replicas.init("nccl", timeout_s=120)
     args.warmup = max(args.warmup, 3)
 
-    if args.impl == "reference":
-        run_reference(args, rank, world)
-        if pg:
-            pg.barrier()
-            pg.destroy_process_group()
-        return
 
     import fcb200 as fcb
     from fcb200 import _lib
@@ -353,8 +347,7 @@ def main():
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    if pg:
-        pg.barrier()
+    replicas.barrier(pg)
     clocks = Clocks(local)
     clocks.start()
     torch.cuda.synchronize()
@@ -366,10 +359,8 @@ def main():
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
-    if pg:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    replicas.barrier(pg)
+    ms = replicas.max_over_ranks(ms, pg, device=dev)
     ms_per_step = ms / args.steps
     value = (ms / 1e3) / (args.steps * world)
     if args.minimal:
@@ -378,9 +369,7 @@ def main():
                               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False,
                               "config": {"cells": list(CELLS), "n": n, "precision": args.precision},
                               "clocks": clk, "minimal": True}), flush=True)
-        if pg:
-            pg.barrier()
-            pg.destroy_process_group()
+        replicas.finalize(pg)
         return
 
     # ---- per-phase device times (profiled pass, same stream, outside the timed region)
@@ -490,9 +479,7 @@ def main():
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    replicas.finalize(pg)
 
 
 if __name__ == "__main__":
