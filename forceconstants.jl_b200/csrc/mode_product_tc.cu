@@ -28,6 +28,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cstdlib>
+
 #include "fcb200_internal.cuh"
 
 namespace fcb {
@@ -409,6 +411,259 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     }
 }
 
+// ---------------------------------------------------------------------------
+// 2-CTA variant (cta_group::2).  A cluster of two CTAs computes a tile of 256
+// rows × up to 256 modes: each CTA stages its own 128 rows of the operand and
+// its half of the φ mode tile, the leader (cluster rank 0) issues
+// tcgen05.mma.cta_group::2 (M = 256) reading both CTAs' shared memory, and
+// each CTA's TMEM receives its 128 rows of the accumulator.  Per SM this moves
+// half as many φ bytes per flop as the 1-CTA tile.  The peer's TMA loads
+// complete on the leader's mbarrier (cp.async.bulk.tensor .cta_group::2, no
+// multicast); the leader's commits multicast to both CTAs' barriers to free
+// their stages and to start both epilogues; the epilogue warps of both CTAs
+// arrive on the leader's accumulator-empty barrier.
+constexpr int STAGES2 = 3;
+constexpr int B2_BYTES = (BN_MAX / 2) * ROW_BYTES;       // half of the mode tile, one plane
+constexpr int STAGE2_BYTES = 2 * A_BYTES + 2 * B2_BYTES;
+constexpr int SMEM2_BYTES = STAGES2 * STAGE2_BYTES + 1024 + 256;
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t mapa_shared(uint32_t addr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar_cluster, int x,
+                                                 int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+        "%3}], [%4];" ::"r"(saddr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar_cluster)
+        : "memory");
+}
+
+template <int KIND>
+__device__ __forceinline__ void umma_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    if constexpr (KIND == 1) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc));
+    }
+}
+
+// arrive on the barrier at this address in both CTAs of the pair
+__device__ __forceinline__ void umma_commit_pair_both(uint64_t* bar) {
+    const uint16_t mask = 0x3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            saddr(bar)),
+        "h"(mask)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit_pair_own(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+    mode_product_tc2_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant__ CUtensorMap mA_lo,
+                            const __grid_constant__ CUtensorMap mB_hi, const __grid_constant__ CUtensorMap mB_lo,
+                            const TcParams p) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES2 * STAGE2_BYTES);
+    uint64_t* empty = full + STAGES2;
+    uint64_t* tfull = empty + STAGES2;
+    uint64_t* tempty = tfull + 2;
+    uint64_t* drain = tempty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES2; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 8);  // 4 epilogue warps in each CTA
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    cluster_sync_all();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int total = p.m_tiles * p.n_tiles;
+    const int half = p.bn / 2;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ------------------------------------------------ TMA producer (both CTAs)
+            int stage = 0;
+            uint32_t phase = 0, filled = 0, filled_phase = 0;
+            bool ok = true;
+            const uint32_t tx_pair = 2u * (2u * A_BYTES + 2u * (uint32_t)half * ROW_BYTES);
+            for (int t = pair; t < total && ok; t += npairs) {
+                const int nt = t % p.n_tiles, mt = t / p.n_tiles;
+                for (int kc = 0; kc < p.k_chunks; ++kc) {
+                    if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_PRODUCER)) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* st = smem + stage * STAGE2_BYTES;
+                    const uint32_t fb = mapa_shared(saddr(&full[stage]), 0);
+                    if (leader) mbar_expect_tx(&full[stage], tx_pair);
+                    const int x = kc * p.elems_per_row;
+                    tma_load_2d_pair(st, &mA_hi, fb, x, mt * 256 + (int)rank * 128);
+                    tma_load_2d_pair(st + A_BYTES, &mA_lo, fb, x, mt * 256 + (int)rank * 128);
+                    tma_load_2d_pair(st + 2 * A_BYTES, &mB_hi, fb, x, nt * p.bn + (int)rank * half);
+                    tma_load_2d_pair(st + 2 * A_BYTES + B2_BYTES, &mB_lo, fb, x, nt * p.bn + (int)rank * half);
+                    filled |= 1u << stage;
+                    filled_phase = (filled_phase & ~(1u << stage)) | (phase << stage);
+                    if (++stage == STAGES2) stage = 0, phase ^= 1;
+                }
+            }
+            if ((!ok || *abort_flag) && leader) {
+                for (int s = 0; s < STAGES2; ++s)
+                    if (filled & (1u << s))
+                        mbar_wait(&full[s], (filled_phase >> s) & 1u, abort_flag, p.status, DEV_TIMEOUT_PRODUCER,
+                                  true);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            // ------------------------------------------------ MMA issuer (leader)
+            const uint32_t idesc = instr_desc<KIND>(256, p.bn);
+            int stage = 0, acc = 0;
+            uint32_t phase = 0, acc_phase = 0;
+            bool ok = true, issued = false;
+            for (int t = pair; t < total && ok; t += npairs) {
+                if (!mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_MMA)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN_MAX);
+                for (int kc = 0; kc < p.k_chunks; ++kc) {
+                    if (!mbar_wait(&full[stage], phase, abort_flag, p.status, DEV_TIMEOUT_MMA)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t base = saddr(smem + stage * STAGE2_BYTES);
+                    const uint64_t a_hi = smem_desc(base), a_lo = smem_desc(base + A_BYTES);
+                    const uint64_t b_hi = smem_desc(base + 2 * A_BYTES);
+                    const uint64_t b_lo = smem_desc(base + 2 * A_BYTES + B2_BYTES);
+#pragma unroll
+                    for (int k = 0; k < ROW_BYTES / 32; ++k) {
+                        const uint64_t off = (uint64_t)((k * 32) >> 4);
+                        umma_pair<KIND>(d_tmem, a_hi + off, b_hi + off, idesc, (kc | k) != 0);
+                        umma_pair<KIND>(d_tmem, a_hi + off, b_lo + off, idesc, 1u);
+                        umma_pair<KIND>(d_tmem, a_lo + off, b_hi + off, idesc, 1u);
+                    }
+                    umma_commit_pair_both(&empty[stage]);
+                    issued = true;
+                    if (++stage == STAGES2) stage = 0, phase ^= 1;
+                }
+                if (!ok) break;
+                umma_commit_pair_both(&tfull[acc]);
+                if (++acc == 2) acc = 0, acc_phase ^= 1;
+            }
+            if ((!ok || *abort_flag) && issued) {
+                umma_commit_pair_own(drain);
+                mbar_wait(drain, 0, abort_flag, p.status, DEV_TIMEOUT_MMA, true);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------------------------------------------- epilogue (both CTAs)
+        const int q = warp & 3;
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        const int chunks = (p.bn + 31) / 32;
+        for (int t = pair; t < total; t += npairs) {
+            const int nt = t % p.n_tiles, mt = t / p.n_tiles;
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait(&tfull[acc], acc_phase, abort_flag, p.status, DEV_TIMEOUT_EPILOGUE);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
+            tc_fence_after();
+            const int64_t row = (int64_t)mt * 256 + rank * 128 + q * 32 + lane;
+            const bool row_ok = row < p.R;
+            const int64_t row_off = row_ok ? (row % p.F) + p.F_pad * (row / p.F) : 0;
+            const int64_t col0 = (int64_t)nt * p.bn;
+            for (int ch = 0; ch < chunks; ++ch) {
+                uint32_t v[32];
+                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN_MAX + ch * 32), v);
+                if (!row_ok) continue;
+                const int64_t c0 = col0 + ch * 32;
+                const int64_t off = row_off + p.ldd * c0;
+                if (ch * 32 + 32 <= p.bn && c0 + 32 <= p.M) {
+                    if (p.out_kind == 1)
+                        store_chunk<1>(p, off, v);
+                    else if (p.out_kind == 0)
+                        store_chunk<0>(p, off, v);
+                    else
+                        store_chunk<2>(p, off, v);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (ch * 32 + j < p.bn && c0 + j < p.M) store_one(p, off + p.ldd * j, __uint_as_float(v[j]));
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(mapa_shared(saddr(&tempty[acc]), 0));
+            if (++acc == 2) acc = 0, acc_phase ^= 1;
+        }
+    }
+
+    tc_fence_before();
+    cluster_sync_all();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
 using EncodeFn = PFN_cuTensorMapEncodeTiled_v12000;
 
 EncodeFn encode_fn() {
@@ -443,10 +698,54 @@ int make_map(CUtensorMap* m, const void* base, int kind, int64_t K, int64_t rows
 
 }  // namespace
 
+// The 2-CTA tile is the default; FCB200_TC_PAIR=0 selects the 1-CTA tile.
+static bool use_pair_kernel() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("FCB200_TC_PAIR");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
 int pad_for(int kind, int64_t n) {
     // TMA needs 16-byte row strides: 8 BF16 or 4 FP32 elements.
     const int64_t q = kind == 1 ? 8 : 4;
     return (int)(((n + q - 1) / q) * q);
+}
+
+// Persistent launch of the 2-CTA kernel: one cluster of two per SM pair, capped
+// by how many such clusters the device can hold at once (GPCs with an odd SM
+// count leave one SM out), so that no cluster waits for another to finish.
+template <typename Kern>
+static int launch_pair(Kern kern, int kind, fcb200_context* h, int64_t tiles, const CUtensorMap& a_hi,
+                       const CUtensorMap& a_lo, const CUtensorMap& b_hi, const CUtensorMap& b_lo, const TcParams& p,
+                       cudaStream_t s) {
+    static int max_clusters[2][64] = {};  // per operand kind and device
+    int& slot = max_clusters[kind - 1][h->device & 63];
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(NUM_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = SMEM2_BYTES;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (slot == 0) {
+        FCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES));
+        cfg.gridDim = dim3(2 * (h->sm_count / 2), 1, 1);
+        int n = 0;
+        FCB_CUDA(cudaOccupancyMaxActiveClusters(&n, kern, &cfg));
+        slot = n > 0 ? n : -1;
+    }
+    if (slot < 0) return set_error(FCB_ERR_UNSUPPORTED, "mode_product_tc: 2-CTA clusters do not fit");
+    const int pairs = (int)(tiles < slot ? tiles : slot);
+    cfg.gridDim = dim3(2 * pairs, 1, 1);
+    FCB_CUDA(cudaLaunchKernelEx(&cfg, kern, a_hi, a_lo, b_hi, b_lo, p));
+    return FCB_OK;
 }
 
 int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A_lo, const void* B_hi,
@@ -480,6 +779,16 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
     FCB_TRY(make_map(&ma_lo, A_lo, kind, mp.K, mp.R, mp.lda, BM));
     FCB_TRY(make_map(&mb_hi, B_hi, kind, mp.K, mp.M, mp.ldb, p.bn));
     FCB_TRY(make_map(&mb_lo, B_lo, kind, mp.K, mp.M, mp.ldb, p.bn));
+    if (use_pair_kernel() && h->sm_count >= 2) {
+        // 2-CTA tiles: 256 rows per pair, each CTA loads half of the mode tile
+        p.m_tiles = (int)((mp.R + 255) / 256);
+        CUtensorMap pb_hi, pb_lo;
+        FCB_TRY(make_map(&pb_hi, B_hi, kind, mp.K, mp.M, mp.ldb, p.bn / 2));
+        FCB_TRY(make_map(&pb_lo, B_lo, kind, mp.K, mp.M, mp.ldb, p.bn / 2));
+        const int64_t tiles2 = (int64_t)p.m_tiles * p.n_tiles;
+        if (kind == 1) return launch_pair(mode_product_tc2_kernel<1>, 1, h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
+        return launch_pair(mode_product_tc2_kernel<2>, 2, h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
+    }
     const int64_t tiles = (int64_t)p.m_tiles * p.n_tiles;
     const int grid = (int)(tiles < h->sm_count ? tiles : h->sm_count);
     if (kind == 1) {
