@@ -257,7 +257,8 @@ int fcb200_trim(fcb200_handle h) {
                    &h->k3_stage[1], &h->ifc2, &h->sw_ints, &h->sw_nbr_r, &h->sw_pair_off, &h->sw_blk3,
                    &h->sw_blk2, &h->sw_atoms, &h->sw_place, &h->sw_col_off, &h->sw_col_items, &h->sw_cursor,
                    &h->sw_asr_off, &h->sw_asr_items, &h->sw_asr, &h->adj_phiT, &h->adj_w_hi, &h->adj_w_lo,
-                   &h->adj_pairs, &h->adj_G, &h->adj_scal, &h->adj_w32, &h->adj_dpos};
+                   &h->adj_pairs, &h->adj_G, &h->adj_scal, &h->adj_w32, &h->adj_dpos, &h->eig_a, &h->eig_w,
+                   &h->eig_work};
     for (Buf* b : bufs) b->release();
     return FCB_OK;
 }
@@ -266,6 +267,7 @@ int fcb200_destroy(fcb200_handle h) {
     if (!h) return FCB_OK;
     cudaSetDevice(h->device);
     fcb200_trim(h);
+    modes_release(h);
     if (h->owns_tune) delete h->tune;
     if (h->d_status) cudaFree(h->d_status);
     if (h->aux_stream) cudaStreamDestroy(h->aux_stream);

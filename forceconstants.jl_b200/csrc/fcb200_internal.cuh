@@ -79,6 +79,9 @@ struct fcb200_context {
     fcb::Buf sw_col_off, sw_col_items, sw_cursor, sw_asr_off, sw_asr_items, sw_asr;
     // adjoint scratch
     fcb::Buf adj_phiT, adj_w_hi, adj_w_lo, adj_pairs, adj_G, adj_scal, adj_w32, adj_dpos;
+    // get_modes: eigensolver handle (cusolverDnHandle_t, opened on first use) and scratch
+    void* solver = nullptr;
+    fcb::Buf eig_a, eig_w, eig_work;
     // Autotuned mode-tile counts per mode-product shape (shared by a handle and
     // its batch lanes; owned by the top-level handle).
     std::unordered_map<uint64_t, int>* tune = nullptr;
@@ -95,6 +98,9 @@ struct fcb200_context {
 namespace fcb {
 
 bool is_device_ptr(const void* p);
+
+// Releases the eigensolver handle of a context (modes.cu).
+void modes_release(fcb200_context* h);
 
 // Key of a mode-product shape in the autotune table.
 inline uint64_t tune_key(int kind, int64_t R, int64_t K, int64_t M) {

@@ -43,6 +43,7 @@ SIGNATURES = {
     "fcb200_third_order_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _D, _P, _P, _P, _I, _P]),
     "fcb200_mass_weight3": (_I, [_P, _P, _P, _I64, _P]),
     "fcb200_second_order_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _D, _P, _P, _P]),
+    "fcb200_get_modes": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P]),
     "fcb200_mcc3": (_I, [_P, _P, _P, _I64, _I64, _I64, _I64, _I64, _I64, _I64, _I, _P, _P]),
     "fcb200_mcc3_blocked": (_I, [_P, _P, _P, _I64, _I64, _I, _P, _P]),
     "fcb200_snapshot_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _D, _P, _P, _I64, _I64, _I, _P, _P, _P]),

@@ -57,7 +57,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
             failed.append(src)
     if failed:
         raise RuntimeError("nvcc failed for: " + ", ".join(os.path.basename(f) for f in failed))
-    link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-ldl"]
     subprocess.run(link, check=True)
     return LIB
 

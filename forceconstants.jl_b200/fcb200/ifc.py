@@ -10,7 +10,7 @@ GPU; there is no CPU path.
 * ``mass_weight_third_order_(ifc3, masses)`` third_order_analytical.jl:185-214
 * ``second_order(sys, pot, calc)``           ifc.jl:3-18
 * ``dynamical_matrix(sys, pot, calc)``       dynmat.jl:5-33
-* ``get_modes(dynmat, n_rigid=3)``           dynmat.jl:123-131
+* ``get_modes(dynmat, n_rigid=3)``           dynmat.jl:123-141 (cuSOLVER syevd on the GPU)
 """
 from __future__ import annotations
 
@@ -130,18 +130,27 @@ def dynamical_matrix(sys: SuperCellSystem, pot, calc, device: str = "cpu") -> De
     return DenseForceConstants(dyn, f"{pot.energy_unit} {pot.length_unit}^-2 u^-1", 0.0)
 
 
-def get_modes(dynmat, num_rigid_translation: int = 3):
-    """dynmat.jl:123-131: ascending eigenpairs of the Hermitian dynamical
-    matrix; the `num_rigid_translation` eigenvalues nearest zero are zeroed.
-    Host LAPACK, as in the reference."""
+def get_modes(dynmat, num_rigid_translation: int = 3, phi32: bool = False):
+    """dynmat.jl:123-141: ascending eigenvalues and orthonormal eigenvectors of
+    the Hermitian dynamical matrix; the ``num_rigid_translation`` eigenvalues
+    nearest zero (stable order of |λ|) are set to 0.  Solved on the GPU
+    (``fcb200_get_modes``, cuSOLVER syevd).  Outputs live where the input
+    lives (numpy in, numpy out; CUDA tensor in, CUDA tensors out).  With
+    ``phi32=True`` the FP32 copy of the eigenvectors — the φ operand of
+    ``mcc3`` — is returned as a third value."""
     vals = dynmat.values if isinstance(dynmat, DenseForceConstants) else dynmat
-    if is_torch(vals):
-        vals = vals.cpu().numpy()
-    w, v = np.linalg.eigh(np.asarray(vals))
-    idx = np.argsort(np.abs(w), kind="stable")
-    w = w.copy()
-    w[idx[:num_rigid_translation]] = 0.0
-    return w, v
+    vals = as_julia(vals, np.float64)
+    if vals.ndim != 2 or vals.shape[0] != vals.shape[1]:
+        raise ValueError("dynmat must be square")
+    n = int(vals.shape[0])
+    dev = device_of(vals)
+    w = julia_empty((n,), np.float64, dev)
+    v = julia_empty((n, n), np.float64, dev)
+    f = julia_empty((n, n), np.float32, dev) if phi32 else None
+    _lib.check(_lib.lib().fcb200_get_modes(
+        _lib.handle(device_index(vals)), ptr(vals), n, int(num_rigid_translation), ptr(w), ptr(v), ptr(f),
+        stream_ptr(vals)))
+    return (w, v, f) if phi32 else (w, v)
 
 
 def asr_satisfied(ifc, n_atoms: int, D: int, tol: float, verbose: bool = False) -> bool:

@@ -119,6 +119,22 @@ int fcb200_second_order_lj(fcb200_handle h, const double* pos, int64_t n_atoms, 
                            const double* masses, double* ifc2_out, void* stream);
 
 /*
+ * Eigen-decomposition of a dynamical matrix on the device.  Replaces
+ * get_modes(dynmat, num_rigid_translation = 3)  src/dynmat.jl:123-141:
+ * ascending eigenvalues (freqs_sq, length n) and orthonormal eigenvectors
+ * (modes, n×n column-major, column c = mode c) of the symmetric n×n FP64
+ * matrix (upper triangle used, as Hermitian(A)); the num_rigid eigenvalues
+ * nearest zero (stable order of |λ|) are set to 0.  phi32 (nullable) receives
+ * the eigenvectors as FP32 — the φ operand of fcb200_mcc3.  modes may be NULL
+ * (vectors discarded) or equal to dynmat (in place).  Any pointer may be host or
+ * device memory.  Synchronises the stream (the solver's convergence flag is
+ * read); a solver that does not converge returns FCB_ERR_CUDA.  Uses
+ * libcusolver, opened on first use (FCB_ERR_UNSUPPORTED when absent).
+ */
+int fcb200_get_modes(fcb200_handle h, const double* dynmat, int64_t n, int num_rigid,
+                     double* freqs_sq, double* modes, float* phi32, void* stream);
+
+/*
  * Dense third-order IFCs of Stillinger-Weber silicon (LAMMPS Si.sw parameters,
  * eV and Å), the AutoDiffCalculator path of the reference.  Replaces
  *   third_order(sys, ::StillingerWeberSilicon, AutoDiffCalculator(tol, r_cut))
