@@ -258,7 +258,7 @@ int fcb200_trim(fcb200_handle h) {
                    &h->sw_blk2, &h->sw_atoms, &h->sw_place, &h->sw_col_off, &h->sw_col_items, &h->sw_cursor,
                    &h->sw_asr_off, &h->sw_asr_items, &h->sw_asr, &h->adj_phiT, &h->adj_w_hi, &h->adj_w_lo,
                    &h->adj_pairs, &h->adj_G, &h->adj_scal, &h->adj_w32, &h->adj_dpos, &h->eig_a, &h->eig_w,
-                   &h->eig_work};
+                   &h->eig_work, &h->sp_ints, &h->sp_coef};
     for (Buf* b : bufs) b->release();
     return FCB_OK;
 }
@@ -601,6 +601,91 @@ int snapshot_run(fcb200_context* h, int64_t N, const float* phi, int64_t mode_lo
     if (host) return check_status(h, s);
     return FCB_OK;
 }
+
+// The LJ snapshot with a block-sparse first mode product (split precisions).
+// Needs the largest neighbour count on the host to size the coefficient
+// tables, so it synchronises the stream once (after the neighbour lists).
+// Sets *used = false, having done nothing visible, when the neighbourhoods are
+// so large that the sparse form does not pay; the caller then runs the dense
+// path.
+int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
+                       double eps, double r_cut, double tol, const double* d_m, const float* phi, int64_t mode_lo,
+                       int64_t mode_hi, int precision, double* psi_out, float* k3_out, cudaStream_t s,
+                       bool host_inputs, bool* used) {
+    *used = false;
+    const int64_t n = 3 * N, M = mode_hi - mode_lo;
+    const int kind = precision == FCB_MCC3_BF16X3 ? 1 : 2;
+    const int64_t np = pad_for(kind, n);
+    const size_t esz = esz_of(kind);
+    float* d_phi;
+    FCB_TRY(device_view(h->phi_f32, phi, (size_t)(n * n), true, s, &d_phi));
+    for (bool& m : h->marked) m = false;
+    phase_mark(h, s, 0);
+    FCB_TRY(lj_pair_tables(h, d_pos, N, d_box, sigma, eps, r_cut, s));
+    phase_mark(h, s, 1);
+    FCB_TRY(h->sp_ints.ensure(sizeof(int) * (size_t)(N * N + 2 * N + 1)));
+    int* d_nb = h->sp_ints.as<int>();
+    int* d_count = d_nb + N * N;
+    int* d_self = d_count + N;
+    int* d_max = d_self + N;
+    FCB_TRY(lj_neighbour_lists(h, N, d_nb, d_count, d_self, d_max, s));
+    int cap = 0;
+    FCB_CUDA(cudaMemcpyAsync(&cap, d_max, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FCB_CUDA(cudaStreamSynchronize(s));
+    cap = (cap + 3) / 4 * 4;  // table stride: a multiple of 4 floats per component
+    // The per-atom tables of the sparse form must fit in shared memory.
+    if (cap < 1 || sparse_p1_smem_bytes(cap, N) > 200 * 1024) return FCB_OK;
+    *used = true;
+    const bool host64 = psi_out && !is_device_ptr(psi_out);
+    double* d_psi64 = psi_out;
+    if (psi_out) {
+        if (host64) {
+            FCB_TRY(h->psi_stage.ensure(sizeof(double) * n * n * n));
+            d_psi64 = h->psi_stage.as<double>();
+        }
+        AssemblyOut out;
+        out.psi64 = d_psi64;
+        FCB_TRY(ifc3_dense_write(h, N, tol, d_m, out, s));
+    }
+    phase_mark(h, s, 2);
+    FCB_TRY(h->sp_coef.ensure(sizeof(float) * (size_t)N * 27 * 3 * cap));
+    FCB_TRY(lj_sparse_coefs(h, N, tol, d_m, d_nb, d_count, d_self, cap, h->sp_coef.as<float>(), s));
+    FCB_TRY(h->phi_hi.ensure(esz * np * n));
+    FCB_TRY(h->phi_lo.ensure(esz * np * n));
+    FCB_TRY(split_operand(d_phi, n, n, n, h->phi_hi.p, h->phi_lo.p, np, kind, s));
+    phase_mark(h, s, 3);
+    FCB_TRY(h->u1_hi.ensure(esz * np * n * M));
+    FCB_TRY(h->u1_lo.ensure(esz * np * n * M));
+    FCB_TRY(sparse_p1_launch(h, kind, N, cap, d_nb, d_count, d_self, h->sp_coef.as<float>(), d_phi, np, mode_lo, M,
+                             h->u1_hi.p, h->u1_lo.p, s));
+    phase_mark(h, s, 4);
+    FCB_TRY(h->u2_hi.ensure(esz * np * M * M));
+    FCB_TRY(h->u2_lo.ensure(esz * np * M * M));
+    auto plane = [&](const Buf& b, int64_t mode) {
+        return static_cast<const void*>(static_cast<const uint8_t*>(b.p) + esz * np * mode);
+    };
+    ModeProduct p2{n * M, n, M, np, np, n, np, np * M};
+    FCB_TRY(mode_product_tc(h, kind, h->u1_hi.p, h->u1_lo.p, plane(h->phi_hi, mode_lo), plane(h->phi_lo, mode_lo),
+                            h->u2_hi.p, h->u2_lo.p, kind, p2, s));
+    phase_mark(h, s, 5);
+    float* d_k3;
+    FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)(M * M * M), false, s, &d_k3));
+    ModeProduct p3{M * M, n, M, np, np, M * M, M * M, M * M};
+    FCB_TRY(mode_product_tc(h, kind, h->u2_hi.p, h->u2_lo.p, plane(h->phi_hi, mode_lo), plane(h->phi_lo, mode_lo),
+                            d_k3, nullptr, 0, p3, s));
+    phase_mark(h, s, 6);
+    bool host = host_inputs || d_phi != phi;
+    if (host64) {
+        FCB_CUDA(cudaMemcpyAsync(psi_out, d_psi64, sizeof(double) * n * n * n, cudaMemcpyDeviceToHost, s));
+        host = true;
+    }
+    if (d_k3 != k3_out) {
+        FCB_CUDA(cudaMemcpyAsync(k3_out, d_k3, sizeof(float) * M * M * M, cudaMemcpyDeviceToHost, s));
+        host = true;
+    }
+    if (host) return check_status(h, s);
+    return FCB_OK;
+}
 }  // namespace
 
 // Device-pointer-only LJ snapshot without validation or host synchronisation
@@ -627,6 +712,8 @@ int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t N, const doub
     if (!phi || !k3_out) return set_error(FCB_ERR_ARG, "phi and k3_out must not be NULL");
     const int64_t n = 3 * N;
     if (!mcc3_ranges_ok(n, mode_lo, mode_hi)) return set_error(FCB_ERR_ARG, "mode window outside [0, n)");
+    const bool force_dense = (precision & FCB_MCC3_FORCE_DENSE) != 0;
+    precision &= ~FCB_MCC3_FORCE_DENSE;
     FCB_TRY(check_precision(precision));
     double bh[3];
     FCB_TRY(box_to_host(box, bh));
@@ -639,6 +726,12 @@ int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t N, const doub
     FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
     FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
     FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
+    if (precision != FCB_MCC3_FP32 && !force_dense) {
+        bool used = false;
+        FCB_TRY(snapshot_lj_sparse(h, d_pos, N, d_box, sigma, eps, r_cut, tol, d_m, phi, mode_lo, mode_hi, precision,
+                                   psi_out, k3_out, s, d_pos != pos, &used));
+        if (used) return FCB_OK;
+    }
     return snapshot_run(h, N, phi, mode_lo, mode_hi, precision, psi_out, k3_out, s, d_pos != pos,
                         [&](const AssemblyOut& out) {
                             FCB_TRY(lj_pair_tables(h, d_pos, N, d_box, sigma, eps, r_cut, s));

@@ -79,6 +79,8 @@ struct fcb200_context {
     fcb::Buf sw_col_off, sw_col_items, sw_cursor, sw_asr_off, sw_asr_items, sw_asr;
     // adjoint scratch
     fcb::Buf adj_phiT, adj_w_hi, adj_w_lo, adj_pairs, adj_G, adj_scal, adj_w32, adj_dpos;
+    // block-sparse P1 of the LJ snapshot: neighbour lists and coefficient tables
+    fcb::Buf sp_ints, sp_coef;
     // get_modes: eigensolver handle (cusolverDnHandle_t, opened on first use) and scratch
     void* solver = nullptr;
     fcb::Buf eig_a, eig_w, eig_work;
@@ -175,6 +177,16 @@ struct ModeProduct {
 
 int mode_product_f32(const float* A, const float* B, float* D, const ModeProduct& mp,
                      cudaStream_t s);
+// Block-sparse first mode product of the LJ snapshot (lj_assembly.cu, sparse_mcc3.cu).
+int lj_neighbour_lists(fcb200_context* h, int64_t N, int* d_nb, int* d_count, int* d_self, int* d_max,
+                       cudaStream_t s);
+int lj_sparse_coefs(fcb200_context* h, int64_t N, double tol, const double* d_masses, const int* d_nb,
+                    const int* d_count, const int* d_self, int cap, float* d_coef, cudaStream_t s);
+size_t sparse_p1_smem_bytes(int cap, int64_t N);
+int sparse_p1_launch(fcb200_context* h, int kind, int64_t N, int cap, const int* d_nb, const int* d_count,
+                     const int* d_self, const float* d_coef, const float* d_phi, int64_t np, int64_t mode_lo,
+                     int64_t M, void* u1_hi, void* u1_lo, cudaStream_t s);
+
 // Split operands (hi/lo planes).  kind 1 = bf16, 2 = tf32 (fp32 planes).
 // out_kind: 0 = fp32 D (D_hi only), 1 = bf16 split D, 2 = tf32 split D.
 int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A_lo,

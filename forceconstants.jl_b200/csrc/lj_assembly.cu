@@ -421,6 +421,76 @@ __global__ void lj_ifc2_kernel(const double* __restrict__ pos, const double* __r
     out[t] = v;
 }
 
+
+// ---------------------------------------------------------------------------
+// Block-sparse first mode product support (snapshot path).
+//
+// For column (j,k) of Ψ with atoms J = j/3, K = k/3 the non-zero rows i lie in
+// atoms {J, K} when J ≠ K (and only when J, K are neighbours), and in the
+// neighbours of K (itself included) when J = K (the ASR column).  So with
+// nbr(K) = {K} ∪ {J : flag(J,K)} every non-zero of the columns k ∈ K lies in
+// rows and columns of nbr(K).
+
+// Ascending neighbour list of every atom (itself included), stride N; the
+// list's length, the self slot, and the largest length over all atoms.
+__global__ void lj_neighbour_list_kernel(const uint8_t* __restrict__ flag, int N, int* __restrict__ nb,
+                                         int* __restrict__ count, int* __restrict__ self_slot,
+                                         int* __restrict__ max_count) {
+    const int lane = threadIdx.x & 31;
+    const int K = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (K >= N) return;
+    int c = 0;
+    for (int J0 = 0; J0 < N; J0 += 32) {
+        const int J = J0 + lane;
+        const bool in = J < N && (J == K || flag[(int64_t)J * N + K]);
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (in) {
+            const int slot = c + __popc(m & ((1u << lane) - 1u));
+            nb[(int64_t)K * N + slot] = J;
+            if (J == K) self_slot[K] = slot;
+        }
+        c += __popc(m);
+    }
+    if (lane == 0) {
+        count[K] = c;
+        atomicMax(max_count, c);
+    }
+}
+
+// Coefficient tables of atom K (FP32, from the final mass-weighted FP64 Ψ):
+//   pair part [kc][t][jl], jl = 3·slot + jc over L = 3·cap entries:
+//       t < 3:  Ψ_mw[3J+t,     3J+jc, 3K+kc]   (J = nbr(K)[slot] ≠ K)
+//       t ≥ 3:  Ψ_mw[3K+t-3,   3J+jc, 3K+kc]
+//   self part [kc][jc][il], il = 3·slot + a:  Ψ_mw[3·nbr(K)[slot]+a, 3K+jc, 3K+kc]
+// Entries past the list (and the pair part of the self slot) are zero.
+__global__ void lj_sparse_coef_kernel(DenseArgs g, const int* __restrict__ nb, const int* __restrict__ count,
+                                      const int* __restrict__ self_slot, int cap, float* __restrict__ coef) {
+    const int K = blockIdx.x;
+    const int N = (int)g.N, L = 3 * cap;
+    const int cnt = count[K], ss = self_slot[K];
+    const int* nbK = nb + (int64_t)K * N;
+    float* out = coef + (int64_t)K * 27 * L;
+    const double mK = g.masses ? g.masses[K] : 0.0;
+    for (int e = threadIdx.x; e < 27 * L; e += blockDim.x) {
+        double raw = 0.0, w = 0.0;
+        if (e < 18 * L) {
+            const int jl = e % L, kt = e / L, kc = kt / 6, t = kt % 6;
+            const int sl = jl / 3, jc = jl % 3;
+            if (sl < cnt && sl != ss) {
+                const int J = nbK[sl];
+                const int I = t < 3 ? J : K, a = t < 3 ? t : t - 3;
+                const double mJ = g.masses ? g.masses[J] : 0.0;
+                finish(g, element_value(g, I, a, J, jc, K, kc), mJ, mK, I, &raw, &w);
+            }
+        } else {
+            const int f = e - 18 * L;
+            const int il = f % L, kj = f / L, kc = kj / 3, jc = kj % 3;
+            const int sl = il / 3, a = il % 3;
+            if (sl < cnt) finish(g, element_value(g, nbK[sl], a, K, jc, K, kc), mK, mK, nbK[sl], &raw, &w);
+        }
+        out[e] = (float)w;
+    }
+}
 }  // namespace
 
 int lj_pair_tables(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
@@ -536,6 +606,33 @@ int ifc3_dense_write_raw(const double* T, const uint8_t* flag, const double* S, 
         ifc3_dense_kernel2<<<(unsigned)blocks, 256, 0, s>>>(g);
     else
         ifc3_dense_kernel<false><<<(unsigned)blocks, 256, 0, s>>>(g);
+    FCB_CUDA(cudaGetLastError());
+    return FCB_OK;
+}
+
+
+int lj_neighbour_lists(fcb200_context* h, int64_t N, int* d_nb, int* d_count, int* d_self, int* d_max,
+                       cudaStream_t s) {
+    FCB_CUDA(cudaMemsetAsync(d_max, 0, sizeof(int), s));
+    const int64_t threads = 32 * N;
+    lj_neighbour_list_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(h->pair_flag.as<uint8_t>(), (int)N,
+                                                                                 d_nb, d_count, d_self, d_max);
+    FCB_CUDA(cudaGetLastError());
+    return FCB_OK;
+}
+
+int lj_sparse_coefs(fcb200_context* h, int64_t N, double tol, const double* d_masses, const int* d_nb,
+                    const int* d_count, const int* d_self, int cap, float* d_coef, cudaStream_t s) {
+    DenseArgs g = {};
+    g.N = N;
+    g.n = 3 * N;
+    g.n_pad = g.n;
+    g.tol = tol;
+    g.T = h->pair_t.as<double>();
+    g.flag = h->pair_flag.as<uint8_t>();
+    g.S = h->self_t.as<double>();
+    g.masses = d_masses;
+    lj_sparse_coef_kernel<<<(unsigned)N, 256, 0, s>>>(g, d_nb, d_count, d_self, cap, d_coef);
     FCB_CUDA(cudaGetLastError());
     return FCB_OK;
 }

@@ -75,11 +75,12 @@ def mcc3_window(psi, phi, n_range, m_range, l_range, precision: str = "fp32"):
 
 
 def snapshot_lj(sys, pot, calc, phi, precision: str = "bf16x3", modes=None, psi_out=None, k3_out=None,
-                stream: int = 0):
+                stream: int = 0, dense: bool = False):
     """Fused third_order → mass_weight_third_order! → Float32 → mcc3 for one
     snapshot (LJ, or Stillinger-Weber when ``pot`` is a
     StillingerWeberSilicon), without the host round trip.  Buffers may be host
-    or device; returns (psi_out, k3_out)."""
+    or device; returns (psi_out, k3_out).  For LJ with a split precision the
+    first two mode products use the block sparsity of Ψ unless ``dense``."""
     from .types import StillingerWeberSilicon
     n = 3 * sys.n_atoms
     lo, hi = (0, n) if modes is None else (int(modes[0]), int(modes[1]))
@@ -96,6 +97,7 @@ def snapshot_lj(sys, pot, calc, phi, precision: str = "bf16x3", modes=None, psi_
         return psi_out, k3_out
     _lib.check(_lib.lib().fcb200_snapshot_lj(
         _lib.handle(dev), ptr(sys.positions), sys.n_atoms, ptr(sys.box_sizes), float(pot.sigma), float(pot.eps),
-        float(calc.r_cut), float(calc.tol), ptr(sys.masses), ptr(phi), lo, hi, _lib.PRECISIONS[precision],
+        float(calc.r_cut), float(calc.tol), ptr(sys.masses), ptr(phi), lo, hi,
+        _lib.PRECISIONS[precision] | (_lib.FCB_MCC3_FORCE_DENSE if dense else 0),
         ptr(psi_out), ptr(k3_out), stream or stream_ptr(k3_out)))
     return psi_out, k3_out

@@ -48,6 +48,9 @@ extern "C" {
 #define FCB_MCC3_FP32       0  /* plain FP32 SIMT mode products (FFMA)                     */
 #define FCB_MCC3_BF16X3     1  /* split-BF16 on tcgen05: hi·hi + hi·lo + lo·hi, FP32 acc   */
 #define FCB_MCC3_TF32X3     2  /* split-TF32 on tcgen05: hi·hi + hi·lo + lo·hi, FP32 acc   */
+/* OR into the precision of fcb200_snapshot_lj: run the dense first and second
+ * mode products even where the block-sparse form applies.                     */
+#define FCB_MCC3_FORCE_DENSE 0x100
 
 /* ---- flags for fcb200_third_order_* -------------------------------------- */
 #define FCB_PSI_MASS_WEIGHTED 1 /* write Ψ already divided by sqrt(m_i m_j m_k) into psi_out */
@@ -197,6 +200,12 @@ int fcb200_mcc3_blocked(fcb200_handle h, const float* psi, const float* phi, int
  *   and mcc3 (src/mcc.jl:29-51)
  * without the host round trip.  psi_out (n³ doubles, unweighted) may be NULL;
  * k3_out holds (mode_hi-mode_lo)³ floats.
+ * With a split precision the first two mode products use the block sparsity of
+ * the LJ Ψ (non-zeros of the columns of atom K lie in rows and columns of K's
+ * neighbourhood): P1 as a sparse contraction, P2 as one GEMM per atom over its
+ * neighbours' degrees of freedom; P3 stays dense.  Same K3 within the mcc3
+ * tolerance; this form synchronises the stream once (after the neighbour
+ * lists).  FCB_MCC3_FORCE_DENSE selects the dense products.
  */
 int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
                        double sigma, double eps, double r_cut, double tol, const double* masses,
