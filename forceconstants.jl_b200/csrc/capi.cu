@@ -130,9 +130,17 @@ struct Mcc3Operand {
 
 // P1..P3 on device buffers.  `emit` receives each finished slab of the last
 // mode axis when slab > 0 (used by the blocked / host-output forms).
+// Symmetric tiles (ModeProduct::sym) are used when the row layout keeps 8
+// consecutive rows contiguous and aligned (the vector epilogue).
+static bool sym_ok(const ModeProduct& mp) { return mp.F % 8 == 0 && mp.F_pad % 8 == 0 && mp.ldd % 8 == 0; }
+
+// `sym`: Ψ is symmetric in all three indices (an assembled IFC3) and the three
+// mode windows coincide, so U2 is symmetric in its two mode indices and K3 in
+// its last two; the tensor-core P2 and P3 then compute only one triangle of
+// tiles and mirror the rest.
 int run_mcc3(fcb200_context* h, int precision, const Mcc3Operand& psi, const float* d_phi, int64_t n,
              int64_t n_lo, int64_t n_hi, int64_t m_lo, int64_t m_hi, int64_t l_lo, int64_t l_hi, float* d_k3,
-             cudaStream_t s) {
+             cudaStream_t s, bool sym = false) {
     const int64_t Mn = n_hi - n_lo, Mm = m_hi - m_lo, Ml = l_hi - l_lo;
     if (precision == FCB_MCC3_FP32) {
         FCB_TRY(h->u1_f32.ensure(sizeof(float) * n * n * Mn));
@@ -168,11 +176,16 @@ int run_mcc3(fcb200_context* h, int precision, const Mcc3Operand& psi, const flo
     FCB_TRY(mode_product_tc(h, kind, psi.hi, psi.lo, plane(h->phi_hi, n_lo), plane(h->phi_lo, n_lo), h->u1_hi.p,
                             h->u1_lo.p, kind, p1, s));
     phase_mark(h, s, 4);
+    sym = sym && n_lo == m_lo && m_lo == l_lo && Mn == Mm && Mm == Ml;
     ModeProduct p2{n * Mn, n, Mm, np, np, n, np, np * Mn};
+    p2.sym = sym && sym_ok(p2);
     FCB_TRY(mode_product_tc(h, kind, h->u1_hi.p, h->u1_lo.p, plane(h->phi_hi, m_lo), plane(h->phi_lo, m_lo),
                             h->u2_hi.p, h->u2_lo.p, kind, p2, s));
     phase_mark(h, s, 5);
     ModeProduct p3{Mn * Mm, n, Ml, np, np, Mn * Mm, Mn * Mm, Mn * Mm};
+    ModeProduct p3s{Mn * Mm, n, Ml, np, np, Mn, Mn, Mn * Mm};  // rows p + Mn·q: K3[p,q,s] = K3[p,s,q]
+    p3s.sym = true;
+    if (sym && sym_ok(p3s)) p3 = p3s;
     FCB_TRY(mode_product_tc(h, kind, h->u2_hi.p, h->u2_lo.p, plane(h->phi_hi, l_lo), plane(h->phi_lo, l_lo), d_k3,
                             nullptr, 0, p3, s));
     phase_mark(h, s, 6);
@@ -588,7 +601,8 @@ int snapshot_run(fcb200_context* h, int64_t N, const float* phi, int64_t mode_lo
     const int64_t M = mode_hi - mode_lo;
     float* d_k3;
     FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)(M * M * M), false, s, &d_k3));
-    FCB_TRY(run_mcc3(h, precision, op, d_phi, n, mode_lo, mode_hi, mode_lo, mode_hi, mode_lo, mode_hi, d_k3, s));
+    FCB_TRY(run_mcc3(h, precision, op, d_phi, n, mode_lo, mode_hi, mode_lo, mode_hi, mode_lo, mode_hi, d_k3, s,
+                     true));
     bool host = host_inputs || d_phi != phi;
     if (host64) {
         FCB_CUDA(cudaMemcpyAsync(psi_out, out.psi64, sizeof(double) * n * n * n, cudaMemcpyDeviceToHost, s));
@@ -664,13 +678,19 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
     auto plane = [&](const Buf& b, int64_t mode) {
         return static_cast<const void*>(static_cast<const uint8_t*>(b.p) + esz * np * mode);
     };
+    // Ψ is symmetric in all three indices: U2[k,p,q] = U2[k,q,p] and
+    // K3[p,q,s] = K3[p,s,q], so P2 and P3 compute one triangle of tiles.
     ModeProduct p2{n * M, n, M, np, np, n, np, np * M};
+    p2.sym = sym_ok(p2);
     FCB_TRY(mode_product_tc(h, kind, h->u1_hi.p, h->u1_lo.p, plane(h->phi_hi, mode_lo), plane(h->phi_lo, mode_lo),
                             h->u2_hi.p, h->u2_lo.p, kind, p2, s));
     phase_mark(h, s, 5);
     float* d_k3;
     FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)(M * M * M), false, s, &d_k3));
     ModeProduct p3{M * M, n, M, np, np, M * M, M * M, M * M};
+    ModeProduct p3s{M * M, n, M, np, np, M, M, M * M};
+    p3s.sym = true;
+    if (sym_ok(p3s)) p3 = p3s;
     FCB_TRY(mode_product_tc(h, kind, h->u2_hi.p, h->u2_lo.p, plane(h->phi_hi, mode_lo), plane(h->phi_lo, mode_lo),
                             d_k3, nullptr, 0, p3, s));
     phase_mark(h, s, 6);

@@ -173,6 +173,11 @@ struct ModeProduct {
     int64_t R, K, M;
     int64_t lda, ldb;
     int64_t F, F_pad, ldd;
+    // Output symmetric under exchanging the row's outer index (r / F) and the
+    // column (e.g. U2[k,p,q] = U2[k,q,p]): tiles whose columns all lie below
+    // their rows' outer index are skipped and every computed entry with
+    // column > outer index is also stored mirrored.  Needs R = F·M rows.
+    bool sym = false;
 };
 
 int mode_product_f32(const float* A, const float* B, float* D, const ModeProduct& mp,

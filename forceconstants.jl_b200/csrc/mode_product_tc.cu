@@ -52,6 +52,8 @@ struct TcParams {
     int64_t F, F_pad, ldd;
     int bn, n_tiles, m_tiles, k_chunks, elems_per_row;
     int out_kind;
+    int sym;  // symmetric output (pair kernel): see ModeProduct::sym
+    int vec;  // F, F_pad, ldd multiples of 8: 8 consecutive rows are 8 consecutive, aligned elements
     void* d_hi;
     void* d_lo;
     int* status;
@@ -234,6 +236,49 @@ __device__ __forceinline__ void store_chunk(const TcParams& p, int64_t off, cons
             dl[j * ldd] = x - h;
         }
     }
+}
+
+// Eight consecutive rows of one column (element offset `off`, a multiple of 8).
+__device__ __forceinline__ void store_vec8(const TcParams& p, int64_t off, const float (&x)[8]) {
+    if (p.out_kind == 1) {
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const __nv_bfloat162 hb = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+            const uint32_t hu = *reinterpret_cast<const uint32_t*>(&hb);
+            const __nv_bfloat162 lb = __floats2bfloat162_rn(x[2 * i] - __uint_as_float(hu << 16),
+                                                            x[2 * i + 1] - __uint_as_float(hu & 0xFFFF0000u));
+            h[i] = hu;
+            l[i] = *reinterpret_cast<const uint32_t*>(&lb);
+        }
+        *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(p.d_hi) + off) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(p.d_lo) + off) = make_uint4(l[0], l[1], l[2], l[3]);
+    } else if (p.out_kind == 0) {
+        float4* d = reinterpret_cast<float4*>(static_cast<float*>(p.d_hi) + off);
+        d[0] = make_float4(x[0], x[1], x[2], x[3]);
+        d[1] = make_float4(x[4], x[5], x[6], x[7]);
+    } else {
+        float hv[8], lv[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            hv[i] = tf32_round(x[i]);
+            lv[i] = x[i] - hv[i];
+        }
+        float4* dh = reinterpret_cast<float4*>(static_cast<float*>(p.d_hi) + off);
+        float4* dl = reinterpret_cast<float4*>(static_cast<float*>(p.d_lo) + off);
+        dh[0] = make_float4(hv[0], hv[1], hv[2], hv[3]);
+        dh[1] = make_float4(hv[4], hv[5], hv[6], hv[7]);
+        dl[0] = make_float4(lv[0], lv[1], lv[2], lv[3]);
+        dl[1] = make_float4(lv[4], lv[5], lv[6], lv[7]);
+    }
+}
+
+// Symmetric output: does pair tile (mt, nt) hold any column >= its rows' outer index?
+__device__ __forceinline__ bool sym_tile_live(const TcParams& p, int mt, int nt) {
+    const int64_t pmin = ((int64_t)mt * 256) / p.F;
+    int64_t qmax = (int64_t)nt * p.bn + p.bn;
+    if (qmax > p.M) qmax = p.M;
+    return qmax - 1 >= pmin;
 }
 
 template <int KIND>
@@ -425,7 +470,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 constexpr int STAGES2 = 3;
 constexpr int B2_BYTES = (BN_MAX / 2) * ROW_BYTES;       // half of the mode tile, one plane
 constexpr int STAGE2_BYTES = 2 * A_BYTES + 2 * B2_BYTES;
-constexpr int SMEM2_BYTES = STAGES2 * STAGE2_BYTES + 1024 + 256;
+// Epilogue staging: per epilogue warp a 32-column × 32-row FP32 block, column
+// stride 36 floats (16-byte aligned rows, conflict-free 128-bit reads).
+constexpr int STG_LD = 36;
+constexpr int STG_BYTES = 4 * 32 * STG_LD * 4;
+constexpr int SMEM2_BYTES = STAGES2 * STAGE2_BYTES + 1024 + 256 + STG_BYTES;
 
 __device__ __forceinline__ uint32_t cluster_rank() {
     uint32_t r;
@@ -500,6 +549,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     uint64_t* drain = tempty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    float* stage_base = reinterpret_cast<float*>(smem + STAGES2 * STAGE2_BYTES + 256);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = cluster_rank();
@@ -541,6 +591,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             const uint32_t tx_pair = 2u * (2u * A_BYTES + 2u * (uint32_t)half * ROW_BYTES);
             for (int t = pair; t < total && ok; t += npairs) {
                 const int nt = t % p.n_tiles, mt = t / p.n_tiles;
+                if (p.sym && !sym_tile_live(p, mt, nt)) continue;
                 for (int kc = 0; kc < p.k_chunks; ++kc) {
                     if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_PRODUCER)) {
                         ok = false;
@@ -575,6 +626,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             uint32_t phase = 0, acc_phase = 0;
             bool ok = true, issued = false;
             for (int t = pair; t < total && ok; t += npairs) {
+                if (p.sym && !sym_tile_live(p, t / p.n_tiles, t % p.n_tiles)) continue;
                 if (!mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_MMA)) {
                     ok = false;
                     break;
@@ -620,6 +672,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         const int chunks = (p.bn + 31) / 32;
         for (int t = pair; t < total; t += npairs) {
             const int nt = t % p.n_tiles, mt = t / p.n_tiles;
+            if (p.sym && !sym_tile_live(p, mt, nt)) continue;
             int ok = 1;
             if (lane == 0) ok = mbar_wait(&tfull[acc], acc_phase, abort_flag, p.status, DEV_TIMEOUT_EPILOGUE);
             ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -629,13 +682,51 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             const bool row_ok = row < p.R;
             const int64_t row_off = row_ok ? (row % p.F) + p.F_pad * (row / p.F) : 0;
             const int64_t col0 = (int64_t)nt * p.bn;
+            const int64_t wrow0 = (int64_t)mt * 256 + rank * 128 + q * 32;  // the warp's first row
+            const bool warp_vec = p.vec && wrow0 + 32 <= p.R;
+            float* stg = stage_base + (warp - 2) * (32 * STG_LD);
             for (int ch = 0; ch < chunks; ++ch) {
                 uint32_t v[32];
                 tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN_MAX + ch * 32), v);
-                if (!row_ok) continue;
                 const int64_t c0 = col0 + ch * 32;
+                if (warp_vec && ch * 32 + 32 <= p.bn && c0 + 32 <= p.M) {
+                    // Transpose the 32×32 block through shared memory so that each
+                    // lane stores 8 consecutive rows of one column as one vector.
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) stg[j * STG_LD + lane] = __uint_as_float(v[j]);
+                    __syncwarp();
+                    const int m = lane & 3;
+                    const int64_t r0 = wrow0 + 8 * m;
+                    const int64_t pr = r0 / p.F, kr = r0 - pr * p.F;
+#pragma unroll
+                    for (int rd = 0; rd < 4; ++rd) {
+                        const int j = 8 * rd + (lane >> 2);
+                        const float4 a = *reinterpret_cast<const float4*>(stg + j * STG_LD + 8 * m);
+                        const float4 b = *reinterpret_cast<const float4*>(stg + j * STG_LD + 8 * m + 4);
+                        const float x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+                        const int64_t qq = c0 + j;
+                        if (!p.sym || qq >= pr) store_vec8(p, kr + p.F_pad * pr + p.ldd * qq, x);
+                        if (p.sym && qq > pr) store_vec8(p, kr + p.F_pad * qq + p.ldd * pr, x);
+                    }
+                    __syncwarp();
+                    continue;
+                }
+                if (!row_ok) continue;
                 const int64_t off = row_off + p.ldd * c0;
-                if (ch * 32 + 32 <= p.bn && c0 + 32 <= p.M) {
+                if (p.sym) {
+                    // direct entries with column q >= p, mirrored ones (k, q, p) with q > p
+                    const int64_t pr = row / p.F, kr = row - pr * p.F;
+                    const int64_t moff = kr + p.ldd * pr + p.F_pad * c0;
+                    const int64_t dlo = pr - c0, mlo = pr + 1 - c0;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        if (ch * 32 + j < p.bn && c0 + j < p.M) {
+                            const float x = __uint_as_float(v[j]);
+                            if (j >= dlo) store_one(p, off + p.ldd * j, x);
+                            if (j >= mlo) store_one(p, moff + p.F_pad * j, x);
+                        }
+                    }
+                } else if (ch * 32 + 32 <= p.bn && c0 + 32 <= p.M) {
                     if (p.out_kind == 1)
                         store_chunk<1>(p, off, v);
                     else if (p.out_kind == 0)
@@ -760,6 +851,9 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
     p.F = mp.F;
     p.F_pad = mp.F_pad;
     p.ldd = mp.ldd;
+    p.sym = mp.sym ? 1 : 0;
+    p.vec = (mp.F % 8 == 0 && mp.F_pad % 8 == 0 && mp.ldd % 8 == 0) ? 1 : 0;
+    if (mp.sym && mp.R != mp.F * mp.M) return set_error(FCB_ERR_ARG, "mode_product_tc: symmetric output needs R = F*M");
     p.n_tiles = (int)((mp.M + BN_MAX - 1) / BN_MAX);
     if (h->tune) {  // autotuned mode-tile count for this shape, if any
         auto it = h->tune->find(tune_key(kind, mp.R, mp.K, mp.M));

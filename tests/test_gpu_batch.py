@@ -1,6 +1,7 @@
 """Batched snapshots (fcb200_batch_*): every K3 of an eager run and of the
-CUDA-graph replays equals the single-snapshot path bit for bit (same kernels,
-same tiles), also after positions change between replays."""
+CUDA-graph replays equals the single-snapshot path with dense mode products
+bit for bit (same kernels, same tiles), also after positions change between
+replays."""
 import numpy as np
 import pytest
 
@@ -28,7 +29,7 @@ def test_batch_matches_single_snapshots(fcb, oracle, cuda_device, precision):
     outs = [b.add(s, pot, calc, p) for s, p in zip(systems, phis)]
 
     def single(s, p):
-        _, k = fcb.snapshot_lj(s, pot, calc, torch.from_numpy(p).cuda(), precision=precision)
+        _, k = fcb.snapshot_lj(s, pot, calc, torch.from_numpy(p).cuda(), precision=precision, dense=True)
         torch.cuda.synchronize()
         return k.cpu().numpy()
 
