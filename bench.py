@@ -41,7 +41,24 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustain
 # DRAM bytes (read + write) per launch at n = 768 from one ncu capture of this
 # command (dram__bytes_read.sum + dram__bytes_write.sum, 1 pass):
 #   mode product (bf16x3): 1.816e9 + 1.767e9; dense IFC3 writer: 0.021e9 + 5.376e9
-NCU_TRAFFIC = {"mode_product_tc_bf16x3": 3.608e9, "ifc3_dense": 5.398e9}
+# DRAM read+write per launch from ncu captures (profiles/); None until captured.
+NCU_TRAFFIC = {"mode_product_tc2_sym": 3.698e9, "ifc3_dense_psi64": 3.570e9}
+
+
+def sym_executed_flops(R, F, K, M, split=3):
+    """Tensor flops one symmetric pair-kernel launch executes: 256-row tiles ×
+    mode tiles of width bn (default tiling: ceil(M/256) tiles), a tile live when
+    its last column reaches its first row's outer index r // F."""
+    n_tiles = -(-M // 256)
+    bn = -(-(-(-M // n_tiles)) // 16) * 16
+    kpad = -(-K // 64) * 64
+    live = 0
+    for mt in range(-(-R // 256)):
+        pmin = (mt * 256) // F
+        for nt in range(n_tiles):
+            if min(nt * bn + bn, M) - 1 >= pmin:
+                live += 1
+    return 2.0 * 256 * bn * kpad * live * split
 
 
 def load_peaks():
@@ -383,17 +400,26 @@ def main():
         acc += np.array(out[:])
     _lib.check(L.fcb200_set_profiling(h, 0))
     phases = acc / reps
-    names = ["pair_tables", "ifc3_dense_write", "phi_split", "mode_product_1", "mode_product_2", "mode_product_3"]
+    split = args.precision != "fp32"
+    if split:
+        names = ["pair_tables", "neighbours_and_ifc3_dense_write", "coefs_and_phi_split", "sparse_mode_product_1",
+                 "mode_product_2", "mode_product_3"]
+    else:
+        names = ["pair_tables", "ifc3_dense_write", "phi_split", "mode_product_1", "mode_product_2", "mode_product_3"]
     phase_ms = {k: round(float(v), 4) for k, v in zip(names, phases)}
 
     peaks, peak_src = load_peaks()
-    split = 3 if args.precision != "fp32" else 1
-    mp_ms = float(np.mean(phases[3:6]))
-    flops_launch = 2.0 * n * n * n * n * split     # R·K·M = n⁴ per product at full modes
-    if args.precision == "fp32":
+    if not split:
+        mp_ms = float(np.mean(phases[3:6]))
+        flops_launch = 2.0 * n ** 4
         roof = {"bound": "fp32-simt", "achieved": flops_launch / (mp_ms * 1e-3) / 1e12, "peak": None,
                 "unit": "TFLOP/s", "frac": None, "traffic": None}
     else:
+        # Dominant kernel: the 2-CTA tensor-core mode product, launched for P2 and P3.
+        # Both run symmetric (one triangle of tiles, mirrored stores); the executed
+        # tensor flops per launch count the live 256-row tiles only, ×3 for the split.
+        mp_ms = float(np.mean(phases[4:6]))
+        flops_launch = float(np.mean([sym_executed_flops(n * n, n, n, n), sym_executed_flops(n * n, n, n, n)]))
         # The step is milliseconds long and the timed region well under a second, so the
         # burst GEMM figure is the denominator; the sustained (power-capped) one is kept beside it.
         pk = peaks["bf16_tflops"] if args.precision == "bf16x3" else None
@@ -402,17 +428,27 @@ def main():
         roof = {"bound": "tensor", "achieved": round(ach, 2), "peak": pk, "unit": "TFLOP/s",
                 "frac": round(ach / pk, 4) if pk else None,
                 "frac_of_sustained": round(ach / pks, 4) if pks else None,
-                "traffic": NCU_TRAFFIC["mode_product_tc_bf16x3"] if (args.precision == "bf16x3" and n == 768) else None,
+                "traffic": NCU_TRAFFIC.get("mode_product_tc2_sym") if (args.precision == "bf16x3" and n == 768) else None,
                 "traffic_unit": "bytes/launch (ncu, DRAM read+write)",
-                "kernel": f"mode_product_tc2_kernel ({args.precision}, 2-CTA tcgen05), 3 launches/step",
+                "kernel": f"mode_product_tc2_kernel ({args.precision}, 2-CTA tcgen05, symmetric tiles), "
+                          "2 launches/step (P2, P3)",
                 "flops_per_launch": flops_launch, "avg_launch_ms": round(mp_ms, 4),
-                "peak_source": f"{peak_src} bf16_tflops (burst; tensor flops executed = 3x useful for the split)"}
-    asm_bytes = 8.0 * n ** 3 + (4.0 if args.precision != "fp32" else 4.0) * n ** 3
+                "useful_flops_per_step": 6.0 * n ** 4,
+                "peak_source": f"{peak_src} bf16_tflops (burst; executed tensor flops = 3x per product for the split)"}
+    asm_bytes = 8.0 * n ** 3 + (0.0 if split else 4.0 * n ** 3)
     asm_ms = float(phases[1])
     roof_asm = {"bound": "hbm", "achieved": round(asm_bytes / (asm_ms * 1e-3) / 1e9, 1), "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": round(asm_bytes / (asm_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4),
-                "traffic": NCU_TRAFFIC["ifc3_dense"] if (args.precision == "bf16x3" and n == 768) else None, "kernel": "ifc3_dense_kernel", "bytes_per_launch": asm_bytes,
-                "avg_launch_ms": round(asm_ms, 4)}
+                "traffic": NCU_TRAFFIC.get("ifc3_dense_psi64") if (split and n == 768) else None,
+                "kernel": "ifc3_dense_kernel2 (FP64 Psi only; the phase also holds the neighbour lists)",
+                "bytes_per_launch": asm_bytes, "avg_launch_ms": round(asm_ms, 4)}
+    sparse_p1 = None
+    if split:
+        u1_bytes = 4.0 * n ** 3          # hi + lo BF16 planes of U1 written
+        p1_ms = float(phases[3])
+        sparse_p1 = {"kernel": "sparse_p1_kernel (CUDA cores, FP32)", "ms": round(p1_ms, 4),
+                     "bytes_written": u1_bytes, "achieved_gbs": round(u1_bytes / (p1_ms * 1e-3) / 1e9, 1),
+                     "frac_of_hbm": round(u1_bytes / (p1_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)}
 
     # ---- accuracy of the timed path vs FP64 (outside timing)
     torch.cuda.synchronize()
@@ -434,6 +470,17 @@ def main():
         torch.cuda.synchronize()
         fp32_s = f0.elapsed_time(f1) / nf / 1e3
         fp32_info = {"s_per_snapshot": fp32_s, "speedup_split_vs_fp32": fp32_s / (ms_per_step / 1e3)}
+        # the same precision with every mode product dense (no sparse P1, no symmetric tiles)
+        dense_prec = prec | _lib.FCB_MCC3_FORCE_DENSE
+        step(precision=dense_prec, k3_ptr=int(k3f.data_ptr()))
+        torch.cuda.synchronize()
+        acc_err[args.precision + "_dense_products"] = err_vs(k3f, ref)
+        f0.record(stream)
+        for _ in range(nf):
+            step(precision=dense_prec, k3_ptr=int(k3f.data_ptr()))
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fp32_info["dense_products_s_per_snapshot"] = f0.elapsed_time(f1) / nf / 1e3
         del k3f
     del ref
     torch.cuda.empty_cache()
@@ -468,7 +515,8 @@ def main():
     if rank == 0 and world == 1 and not args.skip_cpu:
         cpu = cpu_baseline()
 
-    kernels_per_step = 7 if args.precision != "fp32" else 6
+    # split: pair, self, neighbour lists, dense writer, coefficients, phi split, sparse P1, P2, P3
+    kernels_per_step = 9 if split else 6
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
@@ -476,8 +524,10 @@ def main():
         "config": {"workload": "LJ FCC 4x4x4 (256 atoms, n=768), displaced std 0.05 A (seed 1234), "
                                "IFC3 FP64 + mass-weighted split operand, mcc3 all 768 modes",
                    "precision": args.precision, "parallelism": f"replicas x{world}",
-                   "l2": "working set > L2 (Psi64 3.6 GB, intermediates 1.8 GB each); no flush"},
-        "roofline": roof, "roofline_assembly": roof_asm, "phase_ms": phase_ms,
+                   "l2": "working set > L2 (Psi64 3.6 GB, intermediates 1.8 GB each); no flush",
+                   "algorithm": "P1 block-sparse (CUDA cores), P2/P3 symmetric tensor-core tiles" if split
+                   else "dense FP32 mode products"},
+        "roofline": roof, "roofline_assembly": roof_asm, "sparse_p1": sparse_p1, "phase_ms": phase_ms,
         "error_vs_fp64": acc_err, "fp32_gpu": fp32_info, "clocks": clk, "e2e": e2e,
         "cpu_baseline": cpu, "batch": batch, "gpu_launches": kernels_per_step * args.steps,
     }

@@ -689,7 +689,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 uint32_t v[32];
                 tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN_MAX + ch * 32), v);
                 const int64_t c0 = col0 + ch * 32;
-                if (warp_vec && ch * 32 + 32 <= p.bn && c0 + 32 <= p.M) {
+                int64_t ncols = p.M - c0;  // valid columns of this chunk
+                if (ncols > p.bn - ch * 32) ncols = p.bn - ch * 32;
+                if (ncols > 32) ncols = 32;
+                if (warp_vec && ncols > 0) {
                     // Transpose the 32×32 block through shared memory so that each
                     // lane stores 8 consecutive rows of one column as one vector.
 #pragma unroll
@@ -701,6 +704,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 #pragma unroll
                     for (int rd = 0; rd < 4; ++rd) {
                         const int j = 8 * rd + (lane >> 2);
+                        if (j >= ncols) continue;
                         const float4 a = *reinterpret_cast<const float4*>(stg + j * STG_LD + 8 * m);
                         const float4 b = *reinterpret_cast<const float4*>(stg + j * STG_LD + 8 * m + 4);
                         const float x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
