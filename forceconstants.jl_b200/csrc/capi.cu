@@ -8,6 +8,8 @@
 #include <cstring>
 #include <string>
 
+#include <vector>
+
 #include "fcb200_internal.cuh"
 
 namespace fcb {
@@ -87,6 +89,9 @@ int check_status(fcb200_context* h, cudaStream_t s) {
     if (st != DEV_OK) {
         int zero = 0;
         cudaMemcpy(h->d_status, &zero, sizeof(int), cudaMemcpyHostToDevice);
+        if (st == DEV_FD_OVERFLOW)
+            return set_error(FCB_ERR_UNSUPPORTED, "finite differences: more than 128 atoms within the SW cutoff of "
+                                                  "the displaced atoms");
         return set_error(FCB_ERR_TIMEOUT, "a bounded device-side wait gave up (code " + std::to_string(st) +
                                               "); the kernel returned early and its output is invalid");
     }
@@ -271,7 +276,7 @@ int fcb200_trim(fcb200_handle h) {
                    &h->sw_blk2, &h->sw_atoms, &h->sw_place, &h->sw_col_off, &h->sw_col_items, &h->sw_cursor,
                    &h->sw_asr_off, &h->sw_asr_items, &h->sw_asr, &h->adj_phiT, &h->adj_w_hi, &h->adj_w_lo,
                    &h->adj_pairs, &h->adj_G, &h->adj_scal, &h->adj_w32, &h->adj_dpos, &h->eig_a, &h->eig_w,
-                   &h->eig_work, &h->sp_ints, &h->sp_coef};
+                   &h->eig_work, &h->sp_ints, &h->sp_coef, &h->fd_elems, &h->fd_out};
     for (Buf* b : bufs) b->release();
     return FCB_OK;
 }
@@ -821,6 +826,93 @@ int fcb200_snapshot_sw(fcb200_handle h, const double* pos, int64_t N, const doub
                             phase_mark(h, s, 1);
                             return sw_third_order_launch(h, d_pos, N, d_box, r_cut, cos0, tol, d_m, out, s);
                         });
+}
+
+// ---------------------------------------------------------------------------
+// Finite-difference force constants (third_order_FD.jl, second_order_FD.jl).
+
+static int fd_common(fcb200_handle h, const double* pos, int64_t N, const double* box, double step) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    if (!pos || !box) return set_error(FCB_ERR_ARG, "pos and box must not be NULL");
+    if (N < 1 || N > 4096) return set_error(FCB_ERR_ARG, "n_atoms must be in [1, 4096]");
+    if (!(step > 0.0)) return set_error(FCB_ERR_ARG, "the finite-difference step must be positive");
+    return FCB_OK;
+}
+
+static int fd_third(fcb200_handle h, int kind, const double* pos, int64_t N, const double* box, double sigma,
+                    double eps, double r_cut, const int64_t* elems, int64_t m, double step, double* out,
+                    void* stream) {
+    FCB_TRY(fd_common(h, pos, N, box, step));
+    if (m < 0 || (m > 0 && (!elems || !out))) return set_error(FCB_ERR_ARG, "elems and out must hold n_elems entries");
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // The reference asserts the index ranges (third_order_FD.jl:50-51): check them here.
+    std::vector<int64_t> he((size_t)(6 * m));
+    if (m > 0) FCB_CUDA(cudaMemcpy(he.data(), elems, sizeof(int64_t) * 6 * m, cudaMemcpyDefault));
+    for (int64_t e = 0; e < m; ++e)
+        for (int t = 0; t < 3; ++t) {
+            if (he[6 * e + 2 * t] < 0 || he[6 * e + 2 * t] >= N)
+                return set_error(FCB_ERR_ARG, "Atom indexes out of range, must be in 0:" + std::to_string(N - 1));
+            if (he[6 * e + 2 * t + 1] < 0 || he[6 * e + 2 * t + 1] > 2)
+                return set_error(FCB_ERR_ARG, "Cartesian indices must be 0, 1, or 2");
+        }
+    if (m == 0) return FCB_OK;
+    double *d_pos, *d_box, *d_out;
+    int64_t* d_el;
+    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
+    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
+    FCB_TRY(device_view(h->fd_elems, elems, (size_t)(6 * m), true, s, &d_el));
+    FCB_TRY(device_view(h->fd_out, (const double*)out, (size_t)m, false, s, &d_out));
+    FCB_TRY(fd_third_order_launch(d_pos, d_box, N, kind, sigma, eps, r_cut, d_el, m, step, d_out, s));
+    if (d_out != out) {
+        FCB_CUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+        return check_status(h, s);
+    }
+    return FCB_OK;
+}
+
+static int fd_second(fcb200_handle h, int kind, const double* pos, int64_t N, const double* box, double sigma,
+                     double eps, double r_cut, double calc_r_cut, double tol, double step, double* ifc2_out,
+                     void* stream) {
+    FCB_TRY(fd_common(h, pos, N, box, step));
+    if (!ifc2_out) return set_error(FCB_ERR_ARG, "ifc2_out must not be NULL");
+    if (!(calc_r_cut > 0.0)) return set_error(FCB_ERR_ARG, "r_cut must be positive");
+    cudaSetDevice(h->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t n = 3 * N;
+    double *d_pos, *d_box, *d_out;
+    FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
+    FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
+    FCB_TRY(device_view(h->ifc2, (const double*)ifc2_out, (size_t)(n * n), false, s, &d_out));
+    FCB_TRY(fd_second_order_launch(d_pos, d_box, N, kind, sigma, eps, r_cut, calc_r_cut, tol, step, d_out,
+                                   h->d_status, s));
+    if (d_out != ifc2_out)
+        FCB_CUDA(cudaMemcpyAsync(ifc2_out, d_out, sizeof(double) * n * n, cudaMemcpyDeviceToHost, s));
+    return check_status(h, s);
+}
+
+int fcb200_fd_third_order_lj(fcb200_handle h, const double* pos, int64_t N, const double* box, double sigma,
+                             double eps, double r_cut, const int64_t* elems, int64_t n_elems, double step,
+                             double* out, void* stream) {
+    if (!(r_cut > 0.0)) return set_error(FCB_ERR_ARG, "r_cut must be positive");
+    return fd_third(h, 0, pos, N, box, sigma, eps, r_cut, elems, n_elems, step, out, stream);
+}
+
+int fcb200_fd_third_order_sw(fcb200_handle h, const double* pos, int64_t N, const double* box, const int64_t* elems,
+                             int64_t n_elems, double step, double* out, void* stream) {
+    return fd_third(h, 1, pos, N, box, 0.0, 0.0, 0.0, elems, n_elems, step, out, stream);
+}
+
+int fcb200_fd_second_order_lj(fcb200_handle h, const double* pos, int64_t N, const double* box, double sigma,
+                              double eps, double r_cut, double calc_r_cut, double tol, double step, double* ifc2_out,
+                              void* stream) {
+    if (!(r_cut > 0.0)) return set_error(FCB_ERR_ARG, "r_cut must be positive");
+    return fd_second(h, 0, pos, N, box, sigma, eps, r_cut, calc_r_cut, tol, step, ifc2_out, stream);
+}
+
+int fcb200_fd_second_order_sw(fcb200_handle h, const double* pos, int64_t N, const double* box, double calc_r_cut,
+                              double tol, double step, double* ifc2_out, void* stream) {
+    return fd_second(h, 1, pos, N, box, 0.0, 0.0, 0.0, calc_r_cut, tol, step, ifc2_out, stream);
 }
 
 }  // extern "C"

@@ -37,6 +37,7 @@ enum DeviceStatus : int {
     DEV_TIMEOUT_PRODUCER = 1,
     DEV_TIMEOUT_MMA = 2,
     DEV_TIMEOUT_EPILOGUE = 3,
+    DEV_FD_OVERFLOW = 16,  // a finite-difference neighbourhood exceeded its list capacity
 };
 
 // A device buffer cached in a handle and grown on demand.
@@ -81,6 +82,8 @@ struct fcb200_context {
     fcb::Buf adj_phiT, adj_w_hi, adj_w_lo, adj_pairs, adj_G, adj_scal, adj_w32, adj_dpos;
     // block-sparse P1 of the LJ snapshot: neighbour lists and coefficient tables
     fcb::Buf sp_ints, sp_coef;
+    // finite differences: staged element list and output
+    fcb::Buf fd_elems, fd_out;
     // get_modes: eigensolver handle (cusolverDnHandle_t, opened on first use) and scratch
     void* solver = nullptr;
     fcb::Buf eig_a, eig_w, eig_work;
@@ -182,6 +185,13 @@ struct ModeProduct {
 
 int mode_product_f32(const float* A, const float* B, float* D, const ModeProduct& mp,
                      cudaStream_t s);
+// Finite-difference IFCs (finite_diff.cu).  kind 0 = LJ, 1 = SW.
+int fd_third_order_launch(const double* d_pos, const double* d_box, int64_t N, int kind, double sigma, double eps,
+                          double r_cut, const int64_t* d_elems, int64_t m, double h, double* d_out, cudaStream_t s);
+int fd_second_order_launch(const double* d_pos, const double* d_box, int64_t N, int kind, double sigma, double eps,
+                           double r_cut, double calc_r_cut, double tol, double h, double* d_ifc2, int* d_status,
+                           cudaStream_t s);
+
 // Block-sparse first mode product of the LJ snapshot (lj_assembly.cu, sparse_mcc3.cu).
 int lj_neighbour_lists(fcb200_context* h, int64_t N, int* d_nb, int* d_count, int* d_self, int* d_max,
                        cudaStream_t s);

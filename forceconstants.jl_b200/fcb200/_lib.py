@@ -45,6 +45,10 @@ SIGNATURES = {
     "fcb200_mass_weight3": (_I, [_P, _P, _P, _I64, _P]),
     "fcb200_second_order_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _D, _P, _P, _P]),
     "fcb200_get_modes": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P]),
+    "fcb200_fd_third_order_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _P, _I64, _D, _P, _P]),
+    "fcb200_fd_third_order_sw": (_I, [_P, _P, _I64, _P, _P, _I64, _D, _P, _P]),
+    "fcb200_fd_second_order_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _D, _D, _D, _P, _P]),
+    "fcb200_fd_second_order_sw": (_I, [_P, _P, _I64, _P, _D, _D, _D, _P, _P]),
     "fcb200_mcc3": (_I, [_P, _P, _P, _I64, _I64, _I64, _I64, _I64, _I64, _I64, _I, _P, _P]),
     "fcb200_mcc3_blocked": (_I, [_P, _P, _P, _I64, _I64, _I, _P, _P]),
     "fcb200_snapshot_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _D, _P, _P, _I64, _I64, _I, _P, _P, _P]),

@@ -94,6 +94,12 @@ def mass_weight_third_order_(ifc3: DenseForceConstants, masses) -> DenseForceCon
 
 def second_order_(ifc2, sys: SuperCellSystem, pot, calc, n_threads: int | None = None, masses=None):
     del n_threads
+    from .types import FiniteDiffCalculator
+    if isinstance(calc, FiniteDiffCalculator):
+        if masses is not None:
+            raise NotImplementedError("mass weighting of finite-difference IFC2: divide by sqrt(m_i m_j) after")
+        from .finite_diff import second_order_fd_
+        return second_order_fd_(ifc2, sys, pot, calc, device=device_index(ifc2))
     if isinstance(pot, StillingerWeberSilicon):
         from .sw import second_order_sw_
         return second_order_sw_(ifc2, sys, pot, calc, masses=masses)

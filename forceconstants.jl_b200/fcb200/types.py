@@ -122,6 +122,17 @@ class AutoDiffCalculator(ForceConstantCalculator):
     r_cut: float
 
 
+FD_STEP = 0.04 * 0.5291772109   # the reference's default h: 0.04 bohr in Å (types.jl:209)
+
+
+@dataclass
+class FiniteDiffCalculator(ForceConstantCalculator):
+    """types.jl:203-213: (tol, r_cut; h)."""
+    tol: float
+    r_cut: float
+    h: float = FD_STEP
+
+
 @dataclass
 class DenseForceConstants:
     """types.jl:76-80.  ``values`` is a numpy array (host) or a torch tensor

@@ -250,6 +250,38 @@ int fcb200_mcc3_adjoint_lj(fcb200_handle h, const double* pos, int64_t n_atoms, 
 int fcb200_autotune_mcc3(fcb200_handle h, int64_t n, int precision, const char* cache_path, void* stream);
 
 /*
+ * Finite-difference force constants: an independent numerical check of the
+ * analytical (LJ) and AD (SW) assemblies.  Replace
+ *   third_order_finite_diff_eng(sys, pot, atom_idxs, cartesian_idxs; h)
+ *                                   src/finitediff/third_order_FD.jl:43-113
+ *   second_order(sys, pot, FiniteDiffCalculator(tol, r_cut; h))
+ *                                   src/ifc.jl:3-18, src/finitediff/second_order_FD.jl:3-79
+ * with the reference's energy stencils (energy_loop, finitediff_helper.jl:3-64).
+ * elems: n_elems rows of 6 int64 (atom, component) pairs (i,α,j,β,k,γ),
+ * 0-based; out[e] the stencil value, NaN for the arrangements the reference
+ * has no stencil for (i = j != k, j = k != i).  The stencils are the
+ * reference's as written: (i,α,j,β,i,γ) displaces only (i,α) and (j,β); (i,α,
+ * i,β,i,γ) only (i,α).  Each stencil point sums the energy terms that involve
+ * its displaced atoms (the rest cancels because the weights sum to zero).
+ * step: the displacement h in Å (the reference's default is 0.04 bohr =
+ * 0.021167 Å).  LJ energies use the potential's r_cut; the IFC2 pairs are those
+ * within calc_r_cut at the given positions, followed by ASR and apply_tols!(tol).
+ * SW: LAMMPS Si.sw parameters with cosθ₀ = -1/3.  FCB_ERR_UNSUPPORTED when more
+ * than 128 atoms lie within the SW cutoff of a displaced atom.
+ */
+int fcb200_fd_third_order_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                             double sigma, double eps, double r_cut, const int64_t* elems,
+                             int64_t n_elems, double step, double* out, void* stream);
+int fcb200_fd_third_order_sw(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                             const int64_t* elems, int64_t n_elems, double step, double* out,
+                             void* stream);
+int fcb200_fd_second_order_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                              double sigma, double eps, double r_cut, double calc_r_cut, double tol,
+                              double step, double* ifc2_out, void* stream);
+int fcb200_fd_second_order_sw(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
+                              double calc_r_cut, double tol, double step, double* ifc2_out, void* stream);
+
+/*
  * Batches of LJ snapshots (no counterpart in the reference, which runs one
  * snapshot at a time through third_order → mass_weight_third_order! → mcc3,
  * README.md:69-76).  A batch keeps device copies of each snapshot's positions,

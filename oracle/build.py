@@ -15,7 +15,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_OUT = os.path.join(HERE, "_ref")
-SOURCES = ["lj_oracle.c", "sw_oracle.c"]
+SOURCES = ["lj_oracle.c", "sw_oracle.c", "fd_oracle.c"]
 LIB = os.path.join(HERE, "liboracle.so")
 CFLAGS = ["-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-std=c11"]
 

@@ -52,8 +52,45 @@ def lib():
         L.oracle_nearest_mirror.argtypes = [_PD, _PD]
         L.oracle_num_threads.restype = ctypes.c_int
         _sw_signatures(L)
+        _fd_signatures(L)
         _lib = L
     return _lib
+
+
+def _fd_signatures(L):
+    _P64 = ctypes.POINTER(ctypes.c_int64)
+    L.oracle_fd_third_order.argtypes = [ctypes.c_int, _PD, _I64, _PD, _D, _D, _D, _P64, _I64, _D, _PD]
+    L.oracle_fd_second_order.argtypes = [ctypes.c_int, _PD, _I64, _PD, _D, _D, _D, _D, _D, _PD]
+    L.oracle_fd_energy.argtypes = [ctypes.c_int, _PD, _I64, _PD, _D, _D, _D]
+    L.oracle_fd_energy.restype = _D
+
+
+FD_STEP = 0.04 * 0.5291772109   # the reference's default h: 0.04 bohr in Å (third_order_FD.jl:43)
+
+
+def fd_third_order(kind, pos, box, elems, h=FD_STEP, sigma=0.0, eps=0.0, r_cut=0.0):
+    """third_order_finite_diff_eng (src/finitediff/third_order_FD.jl:43-113) for the
+    elements (i, α, j, β, k, γ) (0-based rows of `elems`); kind "lj" or "sw".
+    Total-energy stencils as the reference; NaN where it has none."""
+    pos, N = _pos(pos)
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    e = np.ascontiguousarray(elems, dtype=np.int64).reshape(-1, 6)
+    out = np.empty(e.shape[0])
+    lib().oracle_fd_third_order(0 if kind == "lj" else 1, _pd(pos), N, _pd(box), sigma, eps, r_cut,
+                                e.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), e.shape[0], h, _pd(out))
+    return out
+
+
+def fd_second_order(kind, pos, box, calc_rcut, h=FD_STEP, sigma=0.0, eps=0.0, r_cut=0.0):
+    """second_order! with the FiniteDiffCalculator (src/finitediff/second_order_FD.jl:3-79,
+    ASR src/asr.jl:3-17): n×n column-major."""
+    pos, N = _pos(pos)
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    n = 3 * N
+    out = np.empty(n * n)
+    lib().oracle_fd_second_order(0 if kind == "lj" else 1, _pd(pos), N, _pd(box), sigma, eps, r_cut, calc_rcut,
+                                 h, _pd(out))
+    return out.reshape((n, n), order="F")
 
 
 def _sw_signatures(L):

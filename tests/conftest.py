@@ -46,3 +46,16 @@ def fcc_system(cells, std=0.0, seed=0):
     if std > 0:
         sys_ = fcb200.displaced(sys_, std, seed)
     return sys_
+
+
+def atoms_clear_of_cutoff(sys_, r_cut, margin=0.05):
+    """Atoms with no pair distance (single minimum image) within `margin` of
+    r_cut (the stencils move a pair by at most 2h = 0.042 Å).  A truncated (unshifted) pair energy jumps at r_cut, so a
+    finite-difference stencil that moves such a pair across it measures the
+    jump, in the reference as in any restatement of it."""
+    p = np.asarray(sys_.positions).reshape(-1, 3)
+    d = p[:, None, :] - p[None, :, :]
+    d -= sys_.box_sizes * np.round(d / sys_.box_sizes)
+    dist = np.linalg.norm(d, axis=2)
+    near = (np.abs(dist - r_cut) < margin) & (dist > 0)
+    return np.nonzero(~near.any(axis=1))[0]
