@@ -20,9 +20,9 @@
 namespace fcb {
 namespace {
 
-constexpr int PC = 64;    // modes per CTA
-constexpr int PSUB = 16;  // modes per work item
-constexpr int CJ = 8;     // rows j per chunk (16 bytes of a BF16 plane)
+constexpr int PC = 32;  // modes per CTA
+constexpr int PB = 4;   // modes per shared-memory column block
+constexpr int CJ = 8;   // rows per 16-byte store of a BF16 plane
 
 struct SparseP1Args {
     int N, n, cap, M, mode_lo;
@@ -73,47 +73,43 @@ __device__ __forceinline__ void store_chunk8(void* hi, void* lo, int64_t off, co
     }
 }
 
-// One work item: rows j0 .. j0+7 of the columns (3K+kc, pp0 .. pp0+npp-1).
-// Row j of atom A = j/3 in slot sl of K's list is
-//   Σ_t c[t]·φ[3A+t, p] + Σ_t c[3+t]·φ[3K+t, p]      (A ≠ K),
-//   the self-column sum                               (A = K),
-//   0                                                 (A outside the list).
-__device__ __forceinline__ void chunk_setup(const SparseP1Args& a, const float* cp, const int* slot_of, int L, int ss,
-                                            int j0, int kc, float (&c)[CJ][6], int (&ro)[CJ]) {
-#pragma unroll
-    for (int e = 0; e < CJ; ++e) {
-        const int j = j0 + e;
-        const int A = j / 3, jc = j - 3 * A;
-        const int sl = (j < a.n) ? slot_of[A] : -1;
-        const bool pair = sl >= 0 && sl != ss;
-#pragma unroll
-        for (int t = 0; t < 6; ++t) c[e][t] = pair ? cp[(kc * 6 + t) * L + 3 * sl + jc] : 0.f;
-        ro[e] = 3 * (sl >= 0 ? sl : 0) * (PC + 1);
+template <int KIND>
+__device__ __forceinline__ void store_zero8(void* hi, void* lo, int64_t off, bool tail) {
+    if constexpr (KIND == 1) {
+        *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(hi) + off) = make_uint4(0, 0, 0, 0);
+        *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(lo) + off) = make_uint4(0, 0, 0, 0);
+    } else {
+        float4* ph = reinterpret_cast<float4*>(static_cast<float*>(hi) + off);
+        float4* pl = reinterpret_cast<float4*>(static_cast<float*>(lo) + off);
+        ph[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+        pl[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!tail) {
+            ph[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            pl[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
     }
 }
 
 // One CTA per (atom K, PC modes): the 3·PC columns U1[:, 3K+kc, p].  Shared
-// memory: the φ rows of K's neighbour degrees of freedom for the CTA's modes
-// (row stride PC+1), the atom's coefficient tables, the 9·PC self-column sums,
-// the slot of every atom in K's list (-1 outside) and the column chunks in
-// work order (chunks touching K's neighbourhood first, so that warps stay
-// uniform).
+// memory holds the φ rows of K's neighbourhood for the CTA's modes (row stride
+// PC+1), the atom's coefficient tables, the 9·PC self-column sums, and a block
+// of 3·PB whole columns (n_pad FP32 rows each).  For every PB modes the block is
+// zeroed, the non-zero rows are scattered into it — one thread per (neighbour
+// slot, kc) computes the 3 rows of that atom, 6 terms each — and the block
+// leaves as whole column segments, 8 rows (16 bytes per BF16 plane) per lane.
 template <int KIND>
 __global__ void __launch_bounds__(256) sparse_p1_kernel(SparseP1Args a) {
     extern __shared__ float sm[];
-    __shared__ int n_live;
     const int K = blockIdx.y, p0 = blockIdx.x * PC;
     const int L = 3 * a.cap;
     const int cnt = a.count[K], ss = a.self_slot[K];
-    const int nchunks = (a.n + CJ - 1) / CJ;
+    const int npad = (int)((a.np + CJ - 1) / CJ * CJ);  // block rows: n_pad rounded up to whole chunks
     float* phis = sm;                       // [L][PC+1]
     float* cp = phis + L * (PC + 1);        // pair part [3][6][L], then self part [3][3][L]
     float* cs = cp + 18 * L;
     float* selfres = cp + 27 * L;           // [9][PC]
-    int* slot_of = reinterpret_cast<int*>(selfres + 9 * PC);  // [N]
-    int* order = slot_of + a.N;                                // [nchunks]
+    float* blk = selfres + 9 * PC;          // [3·PB columns][npad] (rows past n stay zero)
     const int* nbK = a.nb + (int64_t)K * a.N;
-    for (int J = threadIdx.x; J < a.N; J += blockDim.x) slot_of[J] = -1;
     for (int il = threadIdx.x; il < L; il += blockDim.x) {
         const int sl = il / 3;
         const bool live = sl < cnt;
@@ -128,30 +124,7 @@ __global__ void __launch_bounds__(256) sparse_p1_kernel(SparseP1Args a) {
         for (int e = threadIdx.x; e < 27 * L / 4; e += blockDim.x) c4[e] = cg[e];
     }
     __syncthreads();
-    for (int sl = threadIdx.x; sl < cnt; sl += blockDim.x) slot_of[nbK[sl]] = sl;
-    __syncthreads();
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp == 0) {
-        int base = 0;
-        for (int pass = 0; pass < 2; ++pass) {
-            for (int c0 = 0; c0 < nchunks; c0 += 32) {
-                const int c = c0 + lane;
-                bool nz = false;
-                if (c < nchunks) {
-                    const int Alo = (c * CJ) / 3, Ahi = (c * CJ + CJ - 1) / 3;
-                    for (int A = Alo; A <= Ahi && A < a.N; ++A) nz |= slot_of[A] >= 0;
-                }
-                const bool want = c < nchunks && (pass == 0 ? nz : !nz);
-                const unsigned m = __ballot_sync(0xffffffffu, want);
-                if (want) order[base + __popc(m & ((1u << lane) - 1u))] = c;
-                base += __popc(m);
-            }
-            if (pass == 0 && lane == 0) n_live = base;
-        }
-    }
-    // Self columns: S[kc·3+jc][pp] = Σ_il cs[kc·3+jc][il]·φ_K[il][pp], one
-    // thread per (pp, group of kj) so that each φ value loaded feeds several sums.
+    // Self columns: S[kc·3+jc][pp] = Σ_il cs[kc·3+jc][il]·φ_K[il][pp].
     for (int o = threadIdx.x; o < 3 * PC; o += blockDim.x) {
         const int pp = o % PC, g = o / PC;  // kj = g, g+3, g+6
         const float* c0 = cs + g * L;
@@ -168,55 +141,67 @@ __global__ void __launch_bounds__(256) sparse_p1_kernel(SparseP1Args a) {
         selfres[(g + 3) * PC + pp] = s1;
         selfres[(g + 6) * PC + pp] = s2;
     }
-    __syncthreads();
-
-    const int items = nchunks * 3 * (PC / PSUB);
-    for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int q = it % nchunks, rest = it / nchunks;
-        const int kc = rest % 3, pp0 = p0 + (rest / 3) * PSUB;
-        if (pp0 >= a.M) continue;
-        const int npp = a.M - pp0 < PSUB ? a.M - pp0 : PSUB;
-        const int j0 = order[q] * CJ;
-        if (q >= n_live) {  // rows outside K's neighbourhood
-            const float z[CJ] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            int64_t off = (int64_t)j0 + a.np * ((int64_t)(3 * K + kc) + (int64_t)a.n * pp0);
-            const int64_t step = a.np * (int64_t)a.n;
-            const bool tail = (int64_t)j0 + 4 >= a.np;
-            for (int pp = 0; pp < npp; ++pp, off += step) store_chunk8<KIND>(a.u1_hi, a.u1_lo, off, z, tail);
-            continue;
-        }
-        float c[CJ][6];
-        int ro[CJ];
-        chunk_setup(a, cp, slot_of, L, ss, j0, kc, c, ro);
-        const float* phK = phis + 3 * ss * (PC + 1);
-        int64_t off = (int64_t)j0 + a.np * ((int64_t)(3 * K + kc) + (int64_t)a.n * pp0);
-        const int64_t step = a.np * (int64_t)a.n;
-        const bool tail = (int64_t)j0 + 4 >= a.np;
-        const int ks = 3 * K - j0;  // position of K's first row in the chunk
-        const bool has_self = ks > -3 && ks < CJ;
-        for (int pp = 0; pp < npp; ++pp, off += step) {
-            const int P = pp0 - p0 + pp;  // mode index within the CTA
-            const float k0 = phK[P], k1 = phK[(PC + 1) + P], k2 = phK[2 * (PC + 1) + P];
-            float v[CJ];
+    const int nch = npad / CJ;              // 16-byte chunks per column
+    const int64_t step = a.np * (int64_t)a.n;
+    for (int pb0 = 0; pb0 < PC && p0 + pb0 < a.M; pb0 += PB) {
+        float4* b4 = reinterpret_cast<float4*>(blk);
+        for (int e = threadIdx.x; e < 3 * PB * npad / 4; e += blockDim.x) b4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        // scatter: item = (slot, kc), the slot's three rows for PB modes
+        for (int it = threadIdx.x; it < 3 * cnt; it += blockDim.x) {
+            const int sl = it / 3, kc = it - 3 * sl;
+            const int J = nbK[sl];
+            if (sl == ss) {
 #pragma unroll
-            for (int e = 0; e < CJ; ++e) {
-                const float* r = phis + ro[e] + P;
-                float acc = c[e][3] * k0;
-                acc = fmaf(c[e][4], k1, acc);
-                acc = fmaf(c[e][5], k2, acc);
-                acc = fmaf(c[e][0], r[0], acc);
-                acc = fmaf(c[e][1], r[PC + 1], acc);
-                v[e] = fmaf(c[e][2], r[2 * (PC + 1)], acc);
+                for (int pb = 0; pb < PB; ++pb)
+#pragma unroll
+                    for (int jc = 0; jc < 3; ++jc)
+                        blk[(kc * PB + pb) * npad + 3 * J + jc] = selfres[(kc * 3 + jc) * PC + pb0 + pb];
+                continue;
             }
-            if (has_self) {
+            float c[3][6];
 #pragma unroll
-                for (int e = 0; e < CJ; ++e) {
-                    const int jc = e - ks;
-                    if (jc >= 0 && jc < 3) v[e] = selfres[(kc * 3 + jc) * PC + P];
+            for (int jc = 0; jc < 3; ++jc)
+#pragma unroll
+                for (int t = 0; t < 6; ++t) c[jc][t] = cp[(kc * 6 + t) * L + 3 * sl + jc];
+            const float* rj = phis + 3 * sl * (PC + 1) + pb0;
+            const float* rk = phis + 3 * ss * (PC + 1) + pb0;
+#pragma unroll
+            for (int pb = 0; pb < PB; ++pb) {
+                const float x0 = rj[pb], x1 = rj[(PC + 1) + pb], x2 = rj[2 * (PC + 1) + pb];
+                const float y0 = rk[pb], y1 = rk[(PC + 1) + pb], y2 = rk[2 * (PC + 1) + pb];
+                float* dst = blk + (kc * PB + pb) * npad + 3 * J;
+#pragma unroll
+                for (int jc = 0; jc < 3; ++jc) {
+                    float acc = c[jc][0] * x0;
+                    acc = fmaf(c[jc][1], x1, acc);
+                    acc = fmaf(c[jc][2], x2, acc);
+                    acc = fmaf(c[jc][3], y0, acc);
+                    acc = fmaf(c[jc][4], y1, acc);
+                    dst[jc] = fmaf(c[jc][5], y2, acc);
                 }
             }
-            store_chunk8<KIND>(a.u1_hi, a.u1_lo, off, v, tail);
         }
+        __syncthreads();
+        // write the block: whole column segments, 8 rows per lane
+        for (int w = threadIdx.x; w < 3 * PB * nch; w += blockDim.x) {
+            const int col = w / nch, c8 = w - col * nch;
+            const int kc = col / PB, pb = col - kc * PB;
+            if (p0 + pb0 + pb >= a.M) continue;
+            const float4 u = *reinterpret_cast<const float4*>(blk + col * npad + CJ * c8);
+            const float4 v = *reinterpret_cast<const float4*>(blk + col * npad + CJ * c8 + 4);
+            const int64_t off = (int64_t)CJ * c8 + a.np * ((int64_t)(3 * K + kc)) + step * (p0 + pb0 + pb);
+            const bool tail = (int64_t)CJ * c8 + 4 >= a.np;
+            const bool zero = u.x == 0.f && u.y == 0.f && u.z == 0.f && u.w == 0.f && v.x == 0.f && v.y == 0.f &&
+                              v.z == 0.f && v.w == 0.f;
+            if (zero) {
+                store_zero8<KIND>(a.u1_hi, a.u1_lo, off, tail);
+            } else {
+                const float x[CJ] = {u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w};
+                store_chunk8<KIND>(a.u1_hi, a.u1_lo, off, x, tail);
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -225,8 +210,8 @@ __global__ void __launch_bounds__(256) sparse_p1_kernel(SparseP1Args a) {
 // cap must be a multiple of 4 (the coefficient tables are copied as float4).
 size_t sparse_p1_smem_bytes(int cap, int64_t N) {
     const size_t L = 3 * (size_t)cap;
-    const size_t nchunks = (3 * (size_t)N + CJ - 1) / CJ;
-    return sizeof(float) * (L * (PC + 1) + 27 * L + 9 * PC) + sizeof(int) * ((size_t)N + nchunks);
+    const size_t npad = (3 * (size_t)N + 7) / 8 * 8;  // the column block holds n_pad rows (≥ the BF16 padding)
+    return sizeof(float) * (L * (PC + 1) + 27 * L + 9 * PC + 3 * PB * npad);
 }
 
 int sparse_p1_launch(fcb200_context* h, int kind, int64_t N, int cap, const int* d_nb, const int* d_count,
