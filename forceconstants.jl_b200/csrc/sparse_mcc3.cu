@@ -143,13 +143,16 @@ __global__ void __launch_bounds__(256) sparse_p1_kernel(SparseP1Args a) {
     }
     const int nch = npad / CJ;              // 16-byte chunks per column
     const int64_t step = a.np * (int64_t)a.n;
-    for (int pb0 = 0; pb0 < PC && p0 + pb0 < a.M; pb0 += PB) {
+    {
         float4* b4 = reinterpret_cast<float4*>(blk);
         for (int e = threadIdx.x; e < 3 * PB * npad / 4; e += blockDim.x) b4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-        __syncthreads();
-        // scatter: item = (slot, kc), the slot's three rows for PB modes
+    }
+    __syncthreads();
+    for (int pb0 = 0; pb0 < PC && p0 + pb0 < a.M; pb0 += PB) {
+        // scatter: item = (slot, kc), slot fastest across lanes (distinct rows,
+        // distinct banks); the block is all zero here
         for (int it = threadIdx.x; it < 3 * cnt; it += blockDim.x) {
-            const int sl = it / 3, kc = it - 3 * sl;
+            const int kc = it / cnt, sl = it - kc * cnt;
             const int J = nbK[sl];
             if (sl == ss) {
 #pragma unroll
@@ -183,13 +186,17 @@ __global__ void __launch_bounds__(256) sparse_p1_kernel(SparseP1Args a) {
             }
         }
         __syncthreads();
-        // write the block: whole column segments, 8 rows per lane
+        // write the block out (whole column segments, 8 rows per lane) and
+        // leave it zero for the next modes
         for (int w = threadIdx.x; w < 3 * PB * nch; w += blockDim.x) {
             const int col = w / nch, c8 = w - col * nch;
             const int kc = col / PB, pb = col - kc * PB;
+            float4* src = reinterpret_cast<float4*>(blk + col * npad + CJ * c8);
+            const float4 u = src[0];
+            const float4 v = src[1];
+            src[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+            src[1] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (p0 + pb0 + pb >= a.M) continue;
-            const float4 u = *reinterpret_cast<const float4*>(blk + col * npad + CJ * c8);
-            const float4 v = *reinterpret_cast<const float4*>(blk + col * npad + CJ * c8 + 4);
             const int64_t off = (int64_t)CJ * c8 + a.np * ((int64_t)(3 * K + kc)) + step * (p0 + pb0 + pb);
             const bool tail = (int64_t)CJ * c8 + 4 >= a.np;
             const bool zero = u.x == 0.f && u.y == 0.f && u.z == 0.f && u.w == 0.f && v.x == 0.f && v.y == 0.f &&
