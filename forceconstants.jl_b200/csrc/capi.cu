@@ -288,6 +288,7 @@ int fcb200_destroy(fcb200_handle h) {
     modes_release(h);
     if (h->owns_tune) delete h->tune;
     if (h->d_status) cudaFree(h->d_status);
+    if (h->h_pinned) cudaFreeHost(h->h_pinned);
     if (h->aux_stream) cudaStreamDestroy(h->aux_stream);
     for (auto& e : h->pev)
         if (e) cudaEventDestroy(e);
@@ -648,13 +649,12 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
     int* d_self = d_count + N;
     int* d_max = d_self + N;
     FCB_TRY(lj_neighbour_lists(h, N, d_nb, d_count, d_self, d_max, s));
-    int cap = 0;
-    FCB_CUDA(cudaMemcpyAsync(&cap, d_max, sizeof(int), cudaMemcpyDeviceToHost, s));
-    FCB_CUDA(cudaStreamSynchronize(s));
-    cap = (cap + 3) / 4 * 4;  // table stride: a multiple of 4 floats per component
-    // The per-atom tables of the sparse form must fit in shared memory.
-    if (cap < 1 || sparse_p1_smem_bytes(cap, N) > 200 * 1024) return FCB_OK;
-    *used = true;
+    // The largest neighbour count sizes the coefficient tables.  It is copied to
+    // pinned memory and waited for through an event, while the FP64 Ψ writer
+    // (which does not need it) already runs, so the GPU does not idle.
+    if (!h->h_pinned) FCB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h->h_pinned), 64));
+    FCB_CUDA(cudaMemcpyAsync(h->h_pinned, d_max, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FCB_CUDA(cudaEventRecord(h->ev[0], s));
     const bool host64 = psi_out && !is_device_ptr(psi_out);
     double* d_psi64 = psi_out;
     if (psi_out) {
@@ -666,6 +666,13 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
         out.psi64 = d_psi64;
         FCB_TRY(ifc3_dense_write(h, N, tol, d_m, out, s));
     }
+    FCB_CUDA(cudaEventSynchronize(h->ev[0]));
+    int cap = h->h_pinned[0];
+    cap = (cap + 3) / 4 * 4;  // table stride: a multiple of 4 floats per component
+    // The per-atom tables of the sparse form must fit in shared memory; if they
+    // do not, the dense path runs (and writes the FP64 Ψ again).
+    if (cap < 1 || sparse_p1_smem_bytes(cap, N) > 200 * 1024) return FCB_OK;
+    *used = true;
     phase_mark(h, s, 2);
     FCB_TRY(h->sp_coef.ensure(sizeof(float) * (size_t)N * 27 * 3 * cap));
     FCB_TRY(lj_sparse_coefs(h, N, tol, d_m, d_nb, d_count, d_self, cap, h->sp_coef.as<float>(), s));

@@ -61,6 +61,7 @@ struct fcb200_context {
     int device = 0;
     int sm_count = 0;
     int* d_status = nullptr;        // device status word (bounded-wait failures)
+    int* h_pinned = nullptr;        // small pinned host buffer for counts read back during a call
     // assembly scratch
     fcb::Buf pos, box, masses;      // staged inputs
     fcb::Buf pair_t, pair_flag;     // per ordered pair: 27 values of -ϕ₃ and a within-cut flag
