@@ -42,7 +42,7 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustain
 # command (dram__bytes_read.sum + dram__bytes_write.sum, 1 pass):
 #   mode product (bf16x3): 1.816e9 + 1.767e9; dense IFC3 writer: 0.021e9 + 5.376e9
 # DRAM read+write per launch from ncu captures (profiles/); None until captured.
-NCU_TRAFFIC = {"mode_product_tc2_sym": 3.698e9, "ifc3_dense_psi64": 3.570e9}
+NCU_TRAFFIC = {"mode_product_tc2_sym": 3.770e9, "ifc3_dense_psi64": 3.570e9}
 
 
 def sym_executed_flops(R, F, K, M, split=3):
