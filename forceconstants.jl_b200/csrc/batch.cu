@@ -28,18 +28,53 @@ namespace {
 struct Snap {
     int64_t N = 0, n = 0;
     double sigma = 0, eps = 0, r_cut = 0, tol = 0;
+    int cap = 0;  // sparse-table capacity (0: dense first mode product)
     Buf pos, box, masses, phi;
     float* k3 = nullptr;
 };
 
-size_t snapshot_footprint(int64_t N, int precision) {
+size_t snapshot_footprint(int64_t N, int precision, int cap) {
     const int64_t n = 3 * N;
     const size_t pair = (size_t)N * N * (27 * 8 + 1) + (size_t)N * 27 * 8;
     if (precision == FCB_MCC3_FP32) return pair + 3 * sizeof(float) * (size_t)n * n * n;
     const int kind = precision == FCB_MCC3_BF16X3 ? 1 : 2;
     const size_t esz = kind == 1 ? 2 : 4;
     const size_t np = (size_t)pad_for(kind, n);
+    if (cap > 0)  // U1, U2 planes, φ planes, coefficient tables, neighbour lists
+        return pair + 2 * esz * np * (size_t)(2 * n * n + n) + sizeof(float) * (size_t)N * 27 * 3 * cap +
+               sizeof(int) * (size_t)(N * N + 2 * N + 1);
     return pair + 2 * esz * np * (size_t)(3 * n * n + n);
+}
+
+// Capacity of the sparse tables for a snapshot: its largest neighbourhood
+// (atoms within r_cut + 0.1 Å by the single minimum image, itself included)
+// plus 4 atoms of headroom, a multiple of 4; 0 selects the dense first mode
+// product (FP32 precision, or tables too large for shared memory).  The
+// headroom lets positions move between replays of the captured graph; a
+// neighbourhood that outgrows it is reported by the status word.
+int host_sparse_cap(const double* pos, int64_t N, const double* box, double r_cut, int precision) {
+    if (precision == FCB_MCC3_FP32) return 0;
+    const double rc = r_cut + 0.1, rc2 = rc * rc;
+    int64_t maxc = 0;
+    for (int64_t K = 0; K < N; ++K) {
+        int64_t c = 1;
+        for (int64_t J = 0; J < N; ++J) {
+            if (J == K) continue;
+            double d2 = 0.0;
+            for (int x = 0; x < 3; ++x) {
+                double r = pos[3 * K + x] - pos[3 * J + x];
+                if (r > box[x] / 2.0) r -= box[x];
+                else if (r < -box[x] / 2.0) r += box[x];
+                d2 += r * r;
+            }
+            if (d2 < rc2) ++c;
+        }
+        maxc = std::max(maxc, c);
+    }
+    int64_t cap = (maxc + 4 + 3) / 4 * 4;
+    if (cap > N) cap = (N + 3) / 4 * 4;
+    if (sparse_p1_smem_bytes((int)cap, N) > 200 * 1024) return 0;
+    return (int)cap;
 }
 
 fcb200_context* child_context(fcb200_context* parent) {
@@ -56,7 +91,8 @@ fcb200_context* child_context(fcb200_context* parent) {
 void release_context(fcb200_context* c) {
     Buf* bufs[] = {&c->pos, &c->box, &c->masses, &c->pair_t, &c->pair_flag, &c->self_t, &c->psi_stage, &c->phi_f32,
                    &c->phi_hi, &c->phi_lo, &c->psi_hi, &c->psi_lo, &c->u1_hi, &c->u1_lo, &c->u2_hi, &c->u2_lo,
-                   &c->u1_f32, &c->u2_f32, &c->psi_f32, &c->k3_stage[0], &c->k3_stage[1]};
+                   &c->u1_f32, &c->u2_f32, &c->psi_f32, &c->k3_stage[0], &c->k3_stage[1], &c->sp_ints,
+                   &c->sp_coef};
     for (Buf* b : bufs) b->release();
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     for (auto& ev : c->ev)
@@ -109,7 +145,7 @@ void drop_lanes(fcb200_batch* b) {
 int make_plan(fcb200_batch* b) {
     drop_lanes(b);
     size_t maxfp = 0;
-    for (auto* s : b->snaps) maxfp = std::max(maxfp, snapshot_footprint(s->N, b->precision));
+    for (auto* s : b->snaps) maxfp = std::max(maxfp, snapshot_footprint(s->N, b->precision, s->cap));
     size_t budget = b->budget;
     if (budget == 0) {
         size_t fr = 0, tot = 0;
@@ -132,7 +168,7 @@ int make_plan(fcb200_batch* b) {
         const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
         const double nn = (double)b->snaps[i]->n;
         load[l] += nn * nn * nn * nn;
-        lane_fp[l] = std::max(lane_fp[l], snapshot_footprint(b->snaps[i]->N, b->precision));
+        lane_fp[l] = std::max(lane_fp[l], snapshot_footprint(b->snaps[i]->N, b->precision, b->snaps[i]->cap));
         b->plan[l].push_back(i);
     }
     b->footprint = 0;
@@ -157,9 +193,14 @@ int issue(fcb200_batch* b, cudaStream_t s) {
         FCB_CUDA(cudaStreamWaitEvent(ls, b->events[0], 0));
         for (int i : b->plan[l]) {
             Snap* sn = b->snaps[i];
-            FCB_TRY(snapshot_lj_device(b->lanes[l], sn->pos.as<double>(), sn->N, sn->box.as<double>(), sn->sigma,
-                                       sn->eps, sn->r_cut, sn->tol, sn->masses.as<double>(), sn->phi.as<float>(), 0,
-                                       sn->n, b->precision, sn->k3, ls));
+            if (sn->cap > 0)
+                FCB_TRY(snapshot_lj_sparse_device(b->lanes[l], sn->pos.as<double>(), sn->N, sn->box.as<double>(),
+                                                  sn->sigma, sn->eps, sn->r_cut, sn->tol, sn->masses.as<double>(),
+                                                  sn->phi.as<float>(), 0, sn->n, b->precision, sn->cap, sn->k3, ls));
+            else
+                FCB_TRY(snapshot_lj_device(b->lanes[l], sn->pos.as<double>(), sn->N, sn->box.as<double>(),
+                                           sn->sigma, sn->eps, sn->r_cut, sn->tol, sn->masses.as<double>(),
+                                           sn->phi.as<float>(), 0, sn->n, b->precision, sn->k3, ls));
         }
         FCB_CUDA(cudaEventRecord(b->events[l + 1], ls));
         FCB_CUDA(cudaStreamWaitEvent(s, b->events[l + 1], 0));
@@ -303,6 +344,11 @@ int fcb200_batch_add_lj(fcb200_batch_t b, const double* pos, int64_t N, const do
         return st;
     }
     FCB_CUDA(cudaMemcpy(s->pos.p, pos, sizeof(double) * 3 * N, cudaMemcpyDefault));
+    {
+        std::vector<double> hp((size_t)(3 * N));
+        FCB_CUDA(cudaMemcpy(hp.data(), pos, sizeof(double) * 3 * N, cudaMemcpyDefault));
+        s->cap = host_sparse_cap(hp.data(), N, bh, r_cut, b->precision);
+    }
     FCB_CUDA(cudaMemcpy(s->box.p, bh, sizeof(double) * 3, cudaMemcpyHostToDevice));
     FCB_CUDA(cudaMemcpy(s->masses.p, masses, sizeof(double) * N, cudaMemcpyDefault));
     FCB_CUDA(cudaMemcpy(s->phi.p, phi, sizeof(float) * s->n * s->n, cudaMemcpyDefault));
@@ -314,6 +360,18 @@ int fcb200_batch_add_lj(fcb200_batch_t b, const double* pos, int64_t N, const do
 int fcb200_batch_set_positions(fcb200_batch_t b, int64_t index, const double* pos, void* stream) {
     if (!b || index < 0 || index >= (int64_t)b->snaps.size() || !pos) return set_error(FCB_ERR_ARG, "bad argument");
     Snap* s = b->snaps[index];
+    if (s->cap > 0) {
+        // a neighbourhood past the sparse tables' capacity re-plans the batch
+        std::vector<double> hp((size_t)(3 * s->N));
+        double bh[3];
+        FCB_CUDA(cudaMemcpy(hp.data(), pos, sizeof(double) * 3 * s->N, cudaMemcpyDefault));
+        FCB_CUDA(cudaMemcpy(bh, s->box.p, sizeof bh, cudaMemcpyDeviceToHost));
+        const int cap = host_sparse_cap(hp.data(), s->N, bh, s->r_cut, b->precision);
+        if (cap == 0 || cap > s->cap) {
+            s->cap = cap;
+            b->dirty = true;
+        }
+    }
     FCB_CUDA(cudaMemcpyAsync(s->pos.p, pos, sizeof(double) * 3 * s->N, cudaMemcpyDefault,
                              static_cast<cudaStream_t>(stream)));
     return FCB_OK;

@@ -89,6 +89,9 @@ int check_status(fcb200_context* h, cudaStream_t s) {
     if (st != DEV_OK) {
         int zero = 0;
         cudaMemcpy(h->d_status, &zero, sizeof(int), cudaMemcpyHostToDevice);
+        if (st == DEV_SPARSE_OVERFLOW)
+            return set_error(FCB_ERR_ARG, "a neighbourhood grew past the capacity fixed when the snapshot was added; "
+                                          "set its positions again so that the batch is re-planned");
         if (st == DEV_FD_OVERFLOW)
             return set_error(FCB_ERR_UNSUPPORTED, "finite differences: more than 128 atoms within the SW cutoff of "
                                                   "the displaced atoms");
@@ -622,6 +625,46 @@ int snapshot_run(fcb200_context* h, int64_t N, const float* phi, int64_t mode_lo
     return FCB_OK;
 }
 
+// Coefficient tables, φ split, sparse P1 and the symmetric P2/P3 (phase marks
+// 3..5; the caller marks 6).
+int sparse_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, int kind, int cap, const int* d_nb,
+                    const int* d_count, const int* d_self, double tol, const double* d_m, const float* d_phi,
+                    float* d_k3, cudaStream_t s) {
+    const int64_t n = 3 * N;
+    const int64_t np = pad_for(kind, n);
+    const size_t esz = esz_of(kind);
+    FCB_TRY(h->sp_coef.ensure(sizeof(float) * (size_t)N * 27 * 3 * cap));
+    FCB_TRY(lj_sparse_coefs(h, N, tol, d_m, d_nb, d_count, d_self, cap, h->sp_coef.as<float>(), s));
+    FCB_TRY(h->phi_hi.ensure(esz * np * n));
+    FCB_TRY(h->phi_lo.ensure(esz * np * n));
+    FCB_TRY(split_operand(d_phi, n, n, n, h->phi_hi.p, h->phi_lo.p, np, kind, s));
+    phase_mark(h, s, 3);
+    FCB_TRY(h->u1_hi.ensure(esz * np * n * M));
+    FCB_TRY(h->u1_lo.ensure(esz * np * n * M));
+    FCB_TRY(sparse_p1_launch(h, kind, N, cap, d_nb, d_count, d_self, h->sp_coef.as<float>(), d_phi, np, mode_lo, M,
+                             h->u1_hi.p, h->u1_lo.p, s));
+    phase_mark(h, s, 4);
+    FCB_TRY(h->u2_hi.ensure(esz * np * M * M));
+    FCB_TRY(h->u2_lo.ensure(esz * np * M * M));
+    auto plane = [&](const Buf& b, int64_t mode) {
+        return static_cast<const void*>(static_cast<const uint8_t*>(b.p) + esz * np * mode);
+    };
+    // Ψ is symmetric in all three indices: U2[k,p,q] = U2[k,q,p] and
+    // K3[p,q,s] = K3[p,s,q], so P2 and P3 compute one triangle of tiles.
+    ModeProduct p2{n * M, n, M, np, np, n, np, np * M};
+    p2.sym = sym_ok(p2);
+    FCB_TRY(mode_product_tc(h, kind, h->u1_hi.p, h->u1_lo.p, plane(h->phi_hi, mode_lo), plane(h->phi_lo, mode_lo),
+                            h->u2_hi.p, h->u2_lo.p, kind, p2, s));
+    phase_mark(h, s, 5);
+    ModeProduct p3{M * M, n, M, np, np, M * M, M * M, M * M};
+    ModeProduct p3s{M * M, n, M, np, np, M, M, M * M};
+    p3s.sym = true;
+    if (sym_ok(p3s)) p3 = p3s;
+    FCB_TRY(mode_product_tc(h, kind, h->u2_hi.p, h->u2_lo.p, plane(h->phi_hi, mode_lo), plane(h->phi_lo, mode_lo),
+                            d_k3, nullptr, 0, p3, s));
+    return FCB_OK;
+}
+
 // The LJ snapshot with a block-sparse first mode product (split precisions).
 // Needs the largest neighbour count on the host to size the coefficient
 // tables, so it synchronises the stream once (after the neighbour lists).
@@ -674,37 +717,9 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
     if (cap < 1 || sparse_p1_smem_bytes(cap, N) > 200 * 1024) return FCB_OK;
     *used = true;
     phase_mark(h, s, 2);
-    FCB_TRY(h->sp_coef.ensure(sizeof(float) * (size_t)N * 27 * 3 * cap));
-    FCB_TRY(lj_sparse_coefs(h, N, tol, d_m, d_nb, d_count, d_self, cap, h->sp_coef.as<float>(), s));
-    FCB_TRY(h->phi_hi.ensure(esz * np * n));
-    FCB_TRY(h->phi_lo.ensure(esz * np * n));
-    FCB_TRY(split_operand(d_phi, n, n, n, h->phi_hi.p, h->phi_lo.p, np, kind, s));
-    phase_mark(h, s, 3);
-    FCB_TRY(h->u1_hi.ensure(esz * np * n * M));
-    FCB_TRY(h->u1_lo.ensure(esz * np * n * M));
-    FCB_TRY(sparse_p1_launch(h, kind, N, cap, d_nb, d_count, d_self, h->sp_coef.as<float>(), d_phi, np, mode_lo, M,
-                             h->u1_hi.p, h->u1_lo.p, s));
-    phase_mark(h, s, 4);
-    FCB_TRY(h->u2_hi.ensure(esz * np * M * M));
-    FCB_TRY(h->u2_lo.ensure(esz * np * M * M));
-    auto plane = [&](const Buf& b, int64_t mode) {
-        return static_cast<const void*>(static_cast<const uint8_t*>(b.p) + esz * np * mode);
-    };
-    // Ψ is symmetric in all three indices: U2[k,p,q] = U2[k,q,p] and
-    // K3[p,q,s] = K3[p,s,q], so P2 and P3 compute one triangle of tiles.
-    ModeProduct p2{n * M, n, M, np, np, n, np, np * M};
-    p2.sym = sym_ok(p2);
-    FCB_TRY(mode_product_tc(h, kind, h->u1_hi.p, h->u1_lo.p, plane(h->phi_hi, mode_lo), plane(h->phi_lo, mode_lo),
-                            h->u2_hi.p, h->u2_lo.p, kind, p2, s));
-    phase_mark(h, s, 5);
     float* d_k3;
     FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)(M * M * M), false, s, &d_k3));
-    ModeProduct p3{M * M, n, M, np, np, M * M, M * M, M * M};
-    ModeProduct p3s{M * M, n, M, np, np, M, M, M * M};
-    p3s.sym = true;
-    if (sym_ok(p3s)) p3 = p3s;
-    FCB_TRY(mode_product_tc(h, kind, h->u2_hi.p, h->u2_lo.p, plane(h->phi_hi, mode_lo), plane(h->phi_lo, mode_lo),
-                            d_k3, nullptr, 0, p3, s));
+    FCB_TRY(sparse_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s));
     phase_mark(h, s, 6);
     bool host = host_inputs || d_phi != phi;
     if (host64) {
@@ -731,6 +746,27 @@ int snapshot_lj_device(fcb200_context* h, const double* d_pos, int64_t N, const 
                             phase_mark(h, s, 1);
                             return ifc3_dense_write(h, N, tol, d_m, out, s);
                         });
+}
+
+int snapshot_lj_sparse_device(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
+                              double eps, double r_cut, double tol, const double* d_m, const float* d_phi,
+                              int64_t mode_lo, int64_t mode_hi, int precision, int cap, float* d_k3, cudaStream_t s) {
+    const int kind = precision == FCB_MCC3_BF16X3 ? 1 : 2;
+    for (bool& m : h->marked) m = false;
+    phase_mark(h, s, 0);
+    FCB_TRY(lj_pair_tables(h, d_pos, N, d_box, sigma, eps, r_cut, s));
+    phase_mark(h, s, 1);
+    FCB_TRY(h->sp_ints.ensure(sizeof(int) * (size_t)(N * N + 2 * N + 1)));
+    int* d_nb = h->sp_ints.as<int>();
+    int* d_count = d_nb + N * N;
+    int* d_self = d_count + N;
+    int* d_max = d_self + N;
+    FCB_TRY(lj_neighbour_lists(h, N, d_nb, d_count, d_self, d_max, s));
+    phase_mark(h, s, 2);
+    FCB_TRY(sparse_products(h, N, mode_lo, mode_hi - mode_lo, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi,
+                            d_k3, s));
+    phase_mark(h, s, 6);
+    return FCB_OK;
 }
 }  // namespace fcb
 

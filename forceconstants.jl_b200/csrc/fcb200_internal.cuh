@@ -38,6 +38,7 @@ enum DeviceStatus : int {
     DEV_TIMEOUT_MMA = 2,
     DEV_TIMEOUT_EPILOGUE = 3,
     DEV_FD_OVERFLOW = 16,  // a finite-difference neighbourhood exceeded its list capacity
+    DEV_SPARSE_OVERFLOW = 17,  // a neighbourhood exceeded the sparse tables' capacity
 };
 
 // A device buffer cached in a handle and grown on demand.
@@ -157,6 +158,12 @@ int sw_second_order_launch(fcb200_context* h, const double* d_pos, int64_t N, co
                            const double* cos0, double tol, const double* d_masses, double* d_ifc2, cudaStream_t s);
 
 // Device-only snapshot (capi.cu), used by the batch engine (batch.cu).
+// Block-sparse LJ snapshot without any host synchronisation: `cap` (a multiple
+// of 4, at least the largest neighbourhood including the atom itself) is fixed
+// by the caller; safe inside stream capture.
+int snapshot_lj_sparse_device(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
+                              double eps, double r_cut, double tol, const double* d_m, const float* d_phi,
+                              int64_t mode_lo, int64_t mode_hi, int precision, int cap, float* d_k3, cudaStream_t s);
 int snapshot_lj_device(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
                        double eps, double r_cut, double tol, const double* d_m, const float* d_phi, int64_t mode_lo,
                        int64_t mode_hi, int precision, float* d_k3, cudaStream_t s);

@@ -464,10 +464,15 @@ __global__ void lj_neighbour_list_kernel(const uint8_t* __restrict__ flag, int N
 //   self part [kc][jc][il], il = 3·slot + a:  Ψ_mw[3·nbr(K)[slot]+a, 3K+jc, 3K+kc]
 // Entries past the list (and the pair part of the self slot) are zero.
 __global__ void lj_sparse_coef_kernel(DenseArgs g, const int* __restrict__ nb, const int* __restrict__ count,
-                                      const int* __restrict__ self_slot, int cap, float* __restrict__ coef) {
+                                      const int* __restrict__ self_slot, int cap, float* __restrict__ coef,
+                                      int* __restrict__ status) {
     const int K = blockIdx.x;
     const int N = (int)g.N, L = 3 * cap;
     const int cnt = count[K], ss = self_slot[K];
+    if (cnt > cap) {  // a capacity fixed in advance was too small: report, write nothing
+        if (threadIdx.x == 0) atomicCAS(status, 0, DEV_SPARSE_OVERFLOW);
+        return;
+    }
     const int* nbK = nb + (int64_t)K * N;
     float* out = coef + (int64_t)K * 27 * L;
     const double mK = g.masses ? g.masses[K] : 0.0;
@@ -632,7 +637,7 @@ int lj_sparse_coefs(fcb200_context* h, int64_t N, double tol, const double* d_ma
     g.flag = h->pair_flag.as<uint8_t>();
     g.S = h->self_t.as<double>();
     g.masses = d_masses;
-    lj_sparse_coef_kernel<<<(unsigned)N, 256, 0, s>>>(g, d_nb, d_count, d_self, cap, d_coef);
+    lj_sparse_coef_kernel<<<(unsigned)N, 256, 0, s>>>(g, d_nb, d_count, d_self, cap, d_coef, h->d_status);
     FCB_CUDA(cudaGetLastError());
     return FCB_OK;
 }

@@ -103,6 +103,7 @@ __global__ void __launch_bounds__(256) sparse_p1_kernel(SparseP1Args a) {
     const int K = blockIdx.y, p0 = blockIdx.x * PC;
     const int L = 3 * a.cap;
     const int cnt = a.count[K], ss = a.self_slot[K];
+    if (cnt > a.cap) return;  // reported by the coefficient kernel; the output is invalid
     const int npad = (int)((a.np + CJ - 1) / CJ * CJ);  // block rows: n_pad rounded up to whole chunks
     float* phis = sm;                       // [L][PC+1]
     float* cp = phis + L * (PC + 1);        // pair part [3][6][L], then self part [3][3][L]

@@ -289,8 +289,13 @@ int fcb200_fd_second_order_sw(fcb200_handle h, const double* pos, int64_t n_atom
  * admitted into up to 4 parallel lanes by HBM footprint (hbm_budget_bytes of
  * scratch; 0 = 80 % of free memory), the first run executes eagerly and sizes
  * every lane's scratch, and every later run replays the whole batch as ONE
- * CUDA-graph launch on `stream`.  Ψ is kept only as the mass-weighted operand
- * of the mode products.  k3_out must be device memory ((3N)³ floats).
+ * CUDA-graph launch on `stream`.  No FP64 Ψ is written.  With a split
+ * precision each snapshot runs the block-sparse first mode product and the
+ * symmetric P2/P3 of fcb200_snapshot_lj; the sparse tables' capacity is fixed
+ * on the host when the snapshot is added (its largest neighbourhood within
+ * r_cut + 0.1 Å, plus 4 atoms) and re-checked by fcb200_batch_set_positions,
+ * which re-plans the batch when positions outgrow it.  k3_out must be device
+ * memory ((3N)³ floats).
  */
 typedef struct fcb200_batch* fcb200_batch_t;
 int fcb200_batch_create(fcb200_handle h, int precision, size_t hbm_budget_bytes, fcb200_batch_t* out);

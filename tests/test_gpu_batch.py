@@ -1,7 +1,8 @@
 """Batched snapshots (fcb200_batch_*): every K3 of an eager run and of the
-CUDA-graph replays equals the single-snapshot path with dense mode products
-bit for bit (same kernels, same tiles), also after positions change between
-replays."""
+CUDA-graph replays equals the single-snapshot path bit for bit (the same
+kernels and tiles: block-sparse first product and symmetric tiles for the
+split precisions, dense FP32 products otherwise), also after positions change
+between replays."""
 import numpy as np
 import pytest
 
@@ -29,7 +30,7 @@ def test_batch_matches_single_snapshots(fcb, oracle, cuda_device, precision):
     outs = [b.add(s, pot, calc, p) for s, p in zip(systems, phis)]
 
     def single(s, p):
-        _, k = fcb.snapshot_lj(s, pot, calc, torch.from_numpy(p).cuda(), precision=precision, dense=True)
+        _, k = fcb.snapshot_lj(s, pot, calc, torch.from_numpy(p).cuda(), precision=precision)
         torch.cuda.synchronize()
         return k.cpu().numpy()
 
@@ -44,7 +45,9 @@ def test_batch_matches_single_snapshots(fcb, oracle, cuda_device, precision):
     b.run()
     torch.cuda.synchronize()
     info = b.info()
-    per_snapshot = 6 if precision == "fp32" else 7      # pair, self, dense, [phi split], 3 mode products
+    # fp32: pair, self, dense writer, 3 mode products; split: pair, self,
+    # neighbour-list memset + kernel, coefficients, phi split, sparse P1, P2, P3
+    per_snapshot = 6 if precision == "fp32" else 9
     assert info["snapshots"] == len(systems) and info["lanes"] >= 1
     assert info["graph_nodes"] >= per_snapshot * len(systems)
     for o, r in zip(outs, ref):
