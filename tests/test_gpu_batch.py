@@ -83,3 +83,28 @@ def test_autotune_cache_roundtrip(fcb, cuda_device, tmp_path):
     assert "mode_tiles" in text
     autotune_mcc3(96, "bf16x3", path)     # cached: no retune, file stays valid
     assert "mode_tiles" in open(path).read()
+
+
+def test_batch_replans_when_neighbourhoods_grow(fcb, oracle, cuda_device):
+    """Positions compressed by 8 % bring more atoms inside the cutoff than the
+    sparse tables were sized for when the snapshot was added; set_positions
+    re-plans the batch, and the result still equals the single-snapshot path."""
+    import torch
+    from fcb200.batch import SnapshotBatch
+    pot = fcb.LJ(AR["sigma"], AR["eps"], AR["r_cut"])
+    calc = fcb.AnalyticalCalculator(1e-12, AR["r_cut"])
+    s = fcc_system((4, 4, 4), 0.03, 41)
+    phi = _phi(oracle, s)
+    b = SnapshotBatch("bf16x3")
+    out = b.add(s, pot, calc, phi)
+    b.run()
+    b.run()
+    b.run()
+    squeezed = fcb.SuperCellSystem(s.positions * 0.92, s.masses, s.box_sizes)
+    b.set_positions(0, squeezed.positions)
+    b.run()
+    torch.cuda.synchronize()
+    _, k = fcb.snapshot_lj(squeezed, pot, calc, torch.from_numpy(phi).cuda(), precision="bf16x3")
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), k.cpu().numpy())
+    b.close()
