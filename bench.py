@@ -402,7 +402,9 @@ def main():
     phases = acc / reps
     split = args.precision != "fp32"
     if split:
-        names = ["pair_tables", "neighbours_and_ifc3_dense_write", "coefs_and_phi_split", "sparse_mode_product_1",
+        # profiled pass: the FP64 writer runs alone inside the second phase; the
+        # timed steps run it beside mode product 2 on a second stream
+        names = ["pair_tables", "neighbours_phi_split_and_ifc3_dense_write", "sparse_coefs", "sparse_mode_product_1",
                  "mode_product_2", "mode_product_3"]
     else:
         names = ["pair_tables", "ifc3_dense_write", "phi_split", "mode_product_1", "mode_product_2", "mode_product_3"]
@@ -440,7 +442,7 @@ def main():
     roof_asm = {"bound": "hbm", "achieved": round(asm_bytes / (asm_ms * 1e-3) / 1e9, 1), "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": round(asm_bytes / (asm_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4),
                 "traffic": NCU_TRAFFIC.get("ifc3_dense_psi64") if (split and n == 768) else None,
-                "kernel": "ifc3_dense_kernel2 (FP64 Psi only; the phase also holds the neighbour lists)",
+                "kernel": "ifc3_dense_kernel2 (FP64 Psi only; the phase also holds the neighbour lists and the phi split)",
                 "bytes_per_launch": asm_bytes, "avg_launch_ms": round(asm_ms, 4)}
     sparse_p1 = None
     if split:
@@ -515,7 +517,8 @@ def main():
     if rank == 0 and world == 1 and not args.skip_cpu:
         cpu = cpu_baseline()
 
-    # split: pair, self, neighbour lists, dense writer, coefficients, phi split, sparse P1, P2, P3
+    # split: pair, self, neighbour lists, phi split, coefficients, sparse P1, P2 with the dense
+    # writer beside it (second stream), P3
     kernels_per_step = 9 if split else 6
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -528,6 +531,10 @@ def main():
                    "algorithm": "P1 block-sparse (CUDA cores), P2/P3 symmetric tensor-core tiles" if split
                    else "dense FP32 mode products"},
         "roofline": roof, "roofline_assembly": roof_asm, "sparse_p1": sparse_p1, "phase_ms": phase_ms,
+        "overlap": ({"phase_sum_ms": round(float(phases.sum()), 4), "ms_per_step": round(ms_per_step, 4),
+                     "saved_ms": round(float(phases.sum()) - ms_per_step, 4),
+                     "note": "phase_ms from a profiled pass with every kernel alone; the timed steps run the "
+                             "FP64 writer on a second stream beside mode product 2"} if split else None),
         "error_vs_fp64": acc_err, "fp32_gpu": fp32_info, "clocks": clk, "e2e": e2e,
         "cpu_baseline": cpu, "batch": batch, "gpu_launches": kernels_per_step * args.steps,
     }

@@ -625,25 +625,34 @@ int snapshot_run(fcb200_context* h, int64_t N, const float* phi, int64_t mode_lo
     return FCB_OK;
 }
 
-// Coefficient tables, φ split, sparse P1 and the symmetric P2/P3 (phase marks
-// 3..5; the caller marks 6).
+// φ in the split layout of the tensor-core products.
+int split_phi(fcb200_context* h, int kind, const float* d_phi, int64_t n, cudaStream_t s) {
+    const int64_t np = pad_for(kind, n);
+    const size_t esz = esz_of(kind);
+    FCB_TRY(h->phi_hi.ensure(esz * np * n));
+    FCB_TRY(h->phi_lo.ensure(esz * np * n));
+    return split_operand(d_phi, n, n, n, h->phi_hi.p, h->phi_lo.p, np, kind, s);
+}
+
+// Coefficient tables, sparse P1 and the symmetric P2/P3 (phase marks 3..5; the
+// caller splits φ before and marks 6 after).  after_p1() is called once P1 is
+// enqueued and before P2.
+template <class AfterP1>
 int sparse_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, int kind, int cap, const int* d_nb,
                     const int* d_count, const int* d_self, double tol, const double* d_m, const float* d_phi,
-                    float* d_k3, cudaStream_t s) {
+                    float* d_k3, cudaStream_t s, AfterP1 after_p1) {
     const int64_t n = 3 * N;
     const int64_t np = pad_for(kind, n);
     const size_t esz = esz_of(kind);
     FCB_TRY(h->sp_coef.ensure(sizeof(float) * (size_t)N * 27 * 3 * cap));
     FCB_TRY(lj_sparse_coefs(h, N, tol, d_m, d_nb, d_count, d_self, cap, h->sp_coef.as<float>(), s));
-    FCB_TRY(h->phi_hi.ensure(esz * np * n));
-    FCB_TRY(h->phi_lo.ensure(esz * np * n));
-    FCB_TRY(split_operand(d_phi, n, n, n, h->phi_hi.p, h->phi_lo.p, np, kind, s));
     phase_mark(h, s, 3);
     FCB_TRY(h->u1_hi.ensure(esz * np * n * M));
     FCB_TRY(h->u1_lo.ensure(esz * np * n * M));
     FCB_TRY(sparse_p1_launch(h, kind, N, cap, d_nb, d_count, d_self, h->sp_coef.as<float>(), d_phi, np, mode_lo, M,
                              h->u1_hi.p, h->u1_lo.p, s));
     phase_mark(h, s, 4);
+    FCB_TRY(after_p1());
     FCB_TRY(h->u2_hi.ensure(esz * np * M * M));
     FCB_TRY(h->u2_lo.ensure(esz * np * M * M));
     auto plane = [&](const Buf& b, int64_t mode) {
@@ -667,10 +676,14 @@ int sparse_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, in
 
 // The LJ snapshot with a block-sparse first mode product (split precisions).
 // Needs the largest neighbour count on the host to size the coefficient
-// tables, so it synchronises the stream once (after the neighbour lists).
-// Sets *used = false, having done nothing visible, when the neighbourhoods are
-// so large that the sparse form does not pay; the caller then runs the dense
-// path.
+// tables, so it synchronises the stream once (after the neighbour lists; the
+// φ split is already queued behind them).  The FP64 Ψ writer (HBM-bound) runs
+// on the aux stream beside P2 and P3 (tensor-core bound), with two blocks per
+// SM so that both kernels stay resident on every SM; the caller's stream waits
+// for it before the end (with phase timing on it runs alone instead, before
+// the sparse products).  Sets *used = false, having done nothing visible, when
+// the neighbourhoods are so large that the sparse form does not pay; the
+// caller then runs the dense path.
 int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
                        double eps, double r_cut, double tol, const double* d_m, const float* phi, int64_t mode_lo,
                        int64_t mode_hi, int precision, double* psi_out, float* k3_out, cudaStream_t s,
@@ -678,8 +691,6 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
     *used = false;
     const int64_t n = 3 * N, M = mode_hi - mode_lo;
     const int kind = precision == FCB_MCC3_BF16X3 ? 1 : 2;
-    const int64_t np = pad_for(kind, n);
-    const size_t esz = esz_of(kind);
     float* d_phi;
     FCB_TRY(device_view(h->phi_f32, phi, (size_t)(n * n), true, s, &d_phi));
     for (bool& m : h->marked) m = false;
@@ -692,19 +703,20 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
     int* d_self = d_count + N;
     int* d_max = d_self + N;
     FCB_TRY(lj_neighbour_lists(h, N, d_nb, d_count, d_self, d_max, s));
-    // The largest neighbour count sizes the coefficient tables.  It is copied to
-    // pinned memory and waited for through an event, while the FP64 Ψ writer
-    // (which does not need it) already runs, so the GPU does not idle.
     if (!h->h_pinned) FCB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h->h_pinned), 64));
     FCB_CUDA(cudaMemcpyAsync(h->h_pinned, d_max, sizeof(int), cudaMemcpyDeviceToHost, s));
     FCB_CUDA(cudaEventRecord(h->ev[0], s));
+    FCB_TRY(split_phi(h, kind, d_phi, n, s));
     const bool host64 = psi_out && !is_device_ptr(psi_out);
     double* d_psi64 = psi_out;
-    if (psi_out) {
-        if (host64) {
-            FCB_TRY(h->psi_stage.ensure(sizeof(double) * n * n * n));
-            d_psi64 = h->psi_stage.as<double>();
-        }
+    if (host64) {
+        FCB_TRY(h->psi_stage.ensure(sizeof(double) * n * n * n));
+        d_psi64 = h->psi_stage.as<double>();
+    }
+    // With phase timing on, the writer runs alone on the caller's stream (full
+    // grid, before the sparse products) so that every phase times one kernel.
+    const bool serial_writer = psi_out && h->profiling;
+    if (serial_writer) {
         AssemblyOut out;
         out.psi64 = d_psi64;
         FCB_TRY(ifc3_dense_write(h, N, tol, d_m, out, s));
@@ -719,7 +731,22 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
     phase_mark(h, s, 2);
     float* d_k3;
     FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)(M * M * M), false, s, &d_k3));
-    FCB_TRY(sparse_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s));
+    bool writer = false;
+    auto launch_writer = [&]() -> int {
+        if (!psi_out || serial_writer) return FCB_OK;
+        FCB_CUDA(cudaEventRecord(h->ev[1], s));
+        FCB_CUDA(cudaStreamWaitEvent(h->aux_stream, h->ev[1], 0));
+        AssemblyOut out;
+        out.psi64 = d_psi64;
+        FCB_TRY(ifc3_dense_write(h, N, tol, d_m, out, h->aux_stream, 2));
+        FCB_CUDA(cudaEventRecord(h->ev[3], h->aux_stream));
+        writer = true;
+        return FCB_OK;
+    };
+    const int rc = sparse_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s,
+                                   launch_writer);
+    if (writer) FCB_CUDA(cudaStreamWaitEvent(s, h->ev[3], 0));
+    FCB_TRY(rc);
     phase_mark(h, s, 6);
     bool host = host_inputs || d_phi != phi;
     if (host64) {
@@ -762,9 +789,10 @@ int snapshot_lj_sparse_device(fcb200_context* h, const double* d_pos, int64_t N,
     int* d_self = d_count + N;
     int* d_max = d_self + N;
     FCB_TRY(lj_neighbour_lists(h, N, d_nb, d_count, d_self, d_max, s));
+    FCB_TRY(split_phi(h, kind, d_phi, 3 * N, s));
     phase_mark(h, s, 2);
     FCB_TRY(sparse_products(h, N, mode_lo, mode_hi - mode_lo, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi,
-                            d_k3, s));
+                            d_k3, s, [] { return (int)FCB_OK; }));
     phase_mark(h, s, 6);
     return FCB_OK;
 }

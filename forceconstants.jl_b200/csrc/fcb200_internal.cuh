@@ -137,8 +137,10 @@ struct AssemblyOut {
 
 int lj_pair_tables(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box,
                    double sigma, double eps, double r_cut, cudaStream_t s);
+// blocks_per_sm caps the grid (grid-stride loop); a small cap leaves room on
+// every SM for a kernel that runs beside the writer on another stream.
 int ifc3_dense_write(fcb200_context* h, int64_t N, double tol, const double* d_masses,
-                     const AssemblyOut& out, cudaStream_t s);
+                     const AssemblyOut& out, cudaStream_t s, int blocks_per_sm = 8);
 int mass_weight3_launch(double* d_psi, const double* d_masses, int64_t N, cudaStream_t s);
 int lj_pair_tables_raw(double* T, uint8_t* flag, double* S, const double* d_pos, int64_t N, const double* d_box,
                        double sigma, double eps, double r_cut, cudaStream_t s);

@@ -517,7 +517,7 @@ int lj_pair_tables(fcb200_context* h, const double* d_pos, int64_t N, const doub
 }
 
 int ifc3_dense_write(fcb200_context* h, int64_t N, double tol, const double* d_masses,
-                     const AssemblyOut& out, cudaStream_t s) {
+                     const AssemblyOut& out, cudaStream_t s, int blocks_per_sm) {
     DenseArgs g;
     g.N = N;
     g.n = 3 * N;
@@ -533,9 +533,20 @@ int ifc3_dense_write(fcb200_context* h, int64_t N, double tol, const double* d_m
     g.split_hi = out.split_hi;
     g.split_lo = out.split_lo;
     g.split_kind = out.split_kind;
+    // The writer asks for the largest shared-memory carveout although it uses
+    // none: an SM whose split was set for a block of the writer must still
+    // take a CTA of the tensor-core mode product (211 KB) running beside it.
+    static bool carveout_set[64] = {};
+    if (h->device >= 0 && h->device < 64 && !carveout_set[h->device]) {
+        FCB_CUDA(cudaFuncSetAttribute(ifc3_dense_kernel2, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared));
+        FCB_CUDA(cudaFuncSetAttribute(ifc3_dense_kernel<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared));
+        carveout_set[h->device] = true;
+    }
     const int64_t cols = g.n * g.n;
     int64_t blocks = (cols + 7) / 8;
-    const int64_t cap = (int64_t)h->sm_count * 8;
+    const int64_t cap = (int64_t)h->sm_count * blocks_per_sm;
     if (blocks > cap) blocks = cap;
     if (g.n % 2 == 0 && g.n_pad % 2 == 0)
         ifc3_dense_kernel2<<<(unsigned)blocks, 256, 0, s>>>(g);
