@@ -38,11 +38,15 @@ UNIT = "s/snapshot"
 CELLS, A_LAT, STD, SEED = (4, 4, 4), 5.2468, 0.05, 1234
 SIGMA, EPS, R_CUT, TOL, MASS = 3.4, 0.24037, 8.5, 1e-12, 39.95
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
-# DRAM bytes (read + write) per launch at n = 768 from one ncu capture of this
-# command (dram__bytes_read.sum + dram__bytes_write.sum, 1 pass):
-#   mode product (bf16x3): 1.816e9 + 1.767e9; dense IFC3 writer: 0.021e9 + 5.376e9
-# DRAM read+write per launch from ncu captures (profiles/); None until captured.
-NCU_TRAFFIC = {"mode_product_tc2_sym": 3.770e9, "ifc3_dense_psi64": 3.570e9}
+# DRAM bytes (read + write) per launch at n = 768, bf16x3, from one 1-pass ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of
+#   python bench.py --steps 2 --warmup 3 --skip-cpu --skip-e2e --skip-batch
+# (profiles/launch_list_snapshot_lj_256atoms_bf16x3.md): the compact form's
+# grouped second product 0.798e9 + 1.753e9, its MN-major third product
+# 1.842e9 + 1.801e9, the FP64 writer 0.006e9 + 3.561e9; the dense-layout
+# symmetric product (taken where the compact form does not pay) 3.770e9.
+NCU_TRAFFIC = {"mode_product_tc2_p2": 2.551e9, "mode_product_tc2_p3": 3.643e9, "mode_product_tc2_sym": 3.770e9,
+               "ifc3_dense_psi64": 3.567e9}
 
 
 def sym_executed_flops(R, F, K, M, split=3):
@@ -59,6 +63,35 @@ def sym_executed_flops(R, F, K, M, split=3):
             if min(nt * bn + bn, M) - 1 >= pmin:
                 live += 1
     return 2.0 * 256 * bn * kpad * live * split
+
+
+def sparse_cap(pos, box, r_cut):
+    """Capacity of the sparse coefficient tables, as the library sizes them for a
+    single snapshot: the largest neighbourhood (atoms within r_cut by the single
+    minimum image, the atom itself included), rounded up to a multiple of 4."""
+    p = np.asarray(pos).reshape(-1, 3)
+    d = p[:, None, :] - p[None, :, :]
+    d -= box * np.round(d / box)
+    cnt = int(((d * d).sum(-1) < r_cut * r_cut).sum(1).max())
+    return -(-cnt // 4) * 4
+
+
+def compact_shapes(n, M, cap):
+    """(Mp, Kc) of the compact sparse products when the library takes that form
+    (modes padded to 256-row blocks, neighbourhood rows to 8; taken when it
+    executes at least 10 % fewer tile flops than the dense-K pair), else None."""
+    if M % 8:
+        return None
+    Mp, Kc = -(-M // 256) * 256, -(-3 * cap // 8) * 8
+    return (Mp, Kc) if Mp * n * Kc + Mp * M * n < 0.9 * (n * M * n + M * M * n) else None
+
+
+def inner_sym_executed_flops(n, M, Mp, Kc, split=3):
+    """Tensor flops of the grouped second product: per column k, 256 × 256 tiles
+    (p, q) with q-tile >= p-tile, K padded to whole 64-wide chunks."""
+    q_tiles = -(-M // 256)
+    live = sum(1 for pt in range(Mp // 256) for qt in range(q_tiles) if min(qt * 256 + 256, M) - 1 >= pt * 256)
+    return 2.0 * 256 * 256 * (-(-Kc // 64) * 64) * live * n * split
 
 
 def load_peaks():
@@ -411,17 +444,26 @@ def main():
     phase_ms = {k: round(float(v), 4) for k, v in zip(names, phases)}
 
     peaks, peak_src = load_peaks()
+    cs = None  # (Mp, Kc) when the compact sparse products run
     if not split:
         mp_ms = float(np.mean(phases[3:6]))
         flops_launch = 2.0 * n ** 4
         roof = {"bound": "fp32-simt", "achieved": flops_launch / (mp_ms * 1e-3) / 1e12, "peak": None,
                 "unit": "TFLOP/s", "frac": None, "traffic": None}
     else:
-        # Dominant kernel: the 2-CTA tensor-core mode product, launched for P2 and P3.
-        # Both run symmetric (one triangle of tiles, mirrored stores); the executed
-        # tensor flops per launch count the live 256-row tiles only, ×3 for the split.
-        mp_ms = float(np.mean(phases[4:6]))
-        flops_launch = float(np.mean([sym_executed_flops(n * n, n, n, n), sym_executed_flops(n * n, n, n, n)]))
+        # Dominant kernel: the 2-CTA tensor-core mode product.  In the compact form
+        # (taken at 256 atoms) it is the third product, reading U2 MN-major with
+        # symmetric tiles; otherwise P2 and P3 both run it with symmetric tiles.
+        # The executed tensor flops count the live 256-row tiles only, ×3 for the split.
+        cs = compact_shapes(n, n, sparse_cap(s.positions, s.box_sizes, R_CUT))
+        if cs:
+            Mp, Kc = cs
+            mp_ms = float(phases[5])
+            flops_launch = sym_executed_flops(Mp * n, Mp, n, n)
+            p2_flops = inner_sym_executed_flops(n, n, Mp, Kc)
+        else:
+            mp_ms = float(np.mean(phases[4:6]))
+            flops_launch = float(np.mean([sym_executed_flops(n * n, n, n, n), sym_executed_flops(n * n, n, n, n)]))
         # The step is milliseconds long and the timed region well under a second, so the
         # burst GEMM figure is the denominator; the sustained (power-capped) one is kept beside it.
         pk = peaks["bf16_tflops"] if args.precision == "bf16x3" else None
@@ -430,13 +472,25 @@ def main():
         roof = {"bound": "tensor", "achieved": round(ach, 2), "peak": pk, "unit": "TFLOP/s",
                 "frac": round(ach / pk, 4) if pk else None,
                 "frac_of_sustained": round(ach / pks, 4) if pks else None,
-                "traffic": NCU_TRAFFIC.get("mode_product_tc2_sym") if (args.precision == "bf16x3" and n == 768) else None,
+                "traffic": NCU_TRAFFIC.get("mode_product_tc2_p3" if cs else "mode_product_tc2_sym")
+                if (args.precision == "bf16x3" and n == 768) else None,
                 "traffic_unit": "bytes/launch (ncu, DRAM read+write)",
-                "kernel": f"mode_product_tc2_kernel ({args.precision}, 2-CTA tcgen05, symmetric tiles), "
-                          "2 launches/step (P2, P3)",
+                "kernel": (f"mode_product_tc2_kernel ({args.precision}, 2-CTA tcgen05, MN-major A, symmetric "
+                           "tiles), the third product" if cs else
+                           f"mode_product_tc2_kernel ({args.precision}, 2-CTA tcgen05, symmetric tiles), "
+                           "2 launches/step (P2, P3)"),
                 "flops_per_launch": flops_launch, "avg_launch_ms": round(mp_ms, 4),
                 "useful_flops_per_step": 6.0 * n ** 4,
                 "peak_source": f"{peak_src} bf16_tflops (burst; executed tensor flops = 3x per product for the split)"}
+        if cs:
+            p2_ms = float(phases[4])
+            a2 = p2_flops / (p2_ms * 1e-3) / 1e12
+            roof["second_product"] = {
+                "kernel": "mode_product_tc2_kernel, grouped by atom (K = Kc), symmetric in (p, q) with transposed "
+                          "stores", "Mp": Mp, "Kc": Kc, "flops_per_launch": p2_flops, "ms": round(p2_ms, 4),
+                "achieved": round(a2, 2), "frac": round(a2 / pk, 4) if pk else None,
+                "traffic": NCU_TRAFFIC.get("mode_product_tc2_p2") if (args.precision == "bf16x3" and n == 768)
+                else None}
     asm_bytes = 8.0 * n ** 3 + (0.0 if split else 4.0 * n ** 3)
     asm_ms = float(phases[1])
     roof_asm = {"bound": "hbm", "achieved": round(asm_bytes / (asm_ms * 1e-3) / 1e9, 1), "peak": peaks["hbm_gbs"],
@@ -446,9 +500,13 @@ def main():
                 "bytes_per_launch": asm_bytes, "avg_launch_ms": round(asm_ms, 4)}
     sparse_p1 = None
     if split:
-        u1_bytes = 4.0 * n ** 3          # hi + lo BF16 planes of U1 written
+        if cs:   # compact U1 and the per-atom φ rows, hi + lo planes
+            u1_bytes = 2.0 * (2 if args.precision == "bf16x3" else 4) * (Mp * n * Kc + s.n_atoms * n * Kc)
+        else:    # hi + lo BF16 planes of the dense-layout U1
+            u1_bytes = 4.0 * n ** 3
         p1_ms = float(phases[3])
-        sparse_p1 = {"kernel": "sparse_p1_kernel (CUDA cores, FP32)", "ms": round(p1_ms, 4),
+        sparse_p1 = {"kernel": "sparse_p1c_kernel (compact, CUDA cores, FP32)" if cs else
+                     "sparse_p1_kernel (CUDA cores, FP32)", "ms": round(p1_ms, 4),
                      "bytes_written": u1_bytes, "achieved_gbs": round(u1_bytes / (p1_ms * 1e-3) / 1e9, 1),
                      "frac_of_hbm": round(u1_bytes / (p1_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)}
 
@@ -528,13 +586,16 @@ def main():
                                "IFC3 FP64 + mass-weighted split operand, mcc3 all 768 modes",
                    "precision": args.precision, "parallelism": f"replicas x{world}",
                    "l2": "working set > L2 (Psi64 3.6 GB, intermediates 1.8 GB each); no flush",
-                   "algorithm": "P1 block-sparse (CUDA cores), P2/P3 symmetric tensor-core tiles" if split
+                   "algorithm": ("P1 neighbourhood-compact (CUDA cores), P2 grouped by atom and P3 MN-major, "
+                                 "both symmetric tensor-core tiles" if cs else
+                                 "P1 block-sparse (CUDA cores), P2/P3 symmetric tensor-core tiles") if split
                    else "dense FP32 mode products"},
         "roofline": roof, "roofline_assembly": roof_asm, "sparse_p1": sparse_p1, "phase_ms": phase_ms,
         "overlap": ({"phase_sum_ms": round(float(phases.sum()), 4), "ms_per_step": round(ms_per_step, 4),
                      "saved_ms": round(float(phases.sum()) - ms_per_step, 4),
                      "note": "phase_ms from a profiled pass with every kernel alone; the timed steps run the "
-                             "FP64 writer on a second stream beside mode product 2"} if split else None),
+                             "FP64 writer on a second stream beside the last tensor-core product(s)"}
+                    if split else None),
         "error_vs_fp64": acc_err, "fp32_gpu": fp32_info, "clocks": clk, "e2e": e2e,
         "cpu_baseline": cpu, "batch": batch, "gpu_launches": kernels_per_step * args.steps,
     }

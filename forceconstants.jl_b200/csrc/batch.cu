@@ -40,9 +40,14 @@ size_t snapshot_footprint(int64_t N, int precision, int cap) {
     const int kind = precision == FCB_MCC3_BF16X3 ? 1 : 2;
     const size_t esz = kind == 1 ? 2 : 4;
     const size_t np = (size_t)pad_for(kind, n);
-    if (cap > 0)  // U1, U2 planes, φ planes, coefficient tables, neighbour lists
-        return pair + 2 * esz * np * (size_t)(2 * n * n + n) + sizeof(float) * (size_t)N * 27 * 3 * cap +
-               sizeof(int) * (size_t)(N * N + 2 * N + 1);
+    if (cap > 0) {  // U1, U2 planes, φ planes, coefficient tables, neighbour lists
+        const size_t tables = sizeof(float) * (size_t)N * 27 * 3 * cap + sizeof(int) * (size_t)(N * N + 2 * N + 1);
+        if (tc_pair_enabled() && compact_pays(n, n, cap)) {  // compact U1, per-atom φ rows, padded U2
+            const size_t Mp = (size_t)compact_Mp(n), Kc = (size_t)compact_Kc(cap);
+            return pair + tables + 2 * esz * (Mp * n * Kc + (size_t)N * n * Kc + Mp * n * n + np * n);
+        }
+        return pair + tables + 2 * esz * np * (size_t)(2 * n * n + n);
+    }
     return pair + 2 * esz * np * (size_t)(3 * n * n + n);
 }
 
@@ -92,7 +97,7 @@ void release_context(fcb200_context* c) {
     Buf* bufs[] = {&c->pos, &c->box, &c->masses, &c->pair_t, &c->pair_flag, &c->self_t, &c->psi_stage, &c->phi_f32,
                    &c->phi_hi, &c->phi_lo, &c->psi_hi, &c->psi_lo, &c->u1_hi, &c->u1_lo, &c->u2_hi, &c->u2_lo,
                    &c->u1_f32, &c->u2_f32, &c->psi_f32, &c->k3_stage[0], &c->k3_stage[1], &c->sp_ints,
-                   &c->sp_coef};
+                   &c->sp_coef, &c->phik_hi, &c->phik_lo};
     for (Buf* b : bufs) b->release();
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     for (auto& ev : c->ev)

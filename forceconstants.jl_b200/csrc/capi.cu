@@ -279,7 +279,7 @@ int fcb200_trim(fcb200_handle h) {
                    &h->sw_blk2, &h->sw_atoms, &h->sw_place, &h->sw_col_off, &h->sw_col_items, &h->sw_cursor,
                    &h->sw_asr_off, &h->sw_asr_items, &h->sw_asr, &h->adj_phiT, &h->adj_w_hi, &h->adj_w_lo,
                    &h->adj_pairs, &h->adj_G, &h->adj_scal, &h->adj_w32, &h->adj_dpos, &h->eig_a, &h->eig_w,
-                   &h->eig_work, &h->sp_ints, &h->sp_coef, &h->fd_elems, &h->fd_out};
+                   &h->eig_work, &h->sp_ints, &h->sp_coef, &h->phik_hi, &h->phik_lo, &h->fd_elems, &h->fd_out};
     for (Buf* b : bufs) b->release();
     return FCB_OK;
 }
@@ -674,12 +674,67 @@ int sparse_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, in
     return FCB_OK;
 }
 
+// Compact form of the sparse products: coefficient tables, the compact first
+// product (U1c and the per-atom φ rows), the grouped second product
+// (U2[p + Mp·k + Mp·n·q], one B per atom, symmetric in (p, q)) and the third
+// product reading U2 MN-major (phase marks 3..5; the caller splits φ before and
+// marks 6 after).  hook() is called before the third product.
+template <class Hook>
+int compact_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, int kind, int cap, const int* d_nb,
+                     const int* d_count, const int* d_self, double tol, const double* d_m, const float* d_phi,
+                     float* d_k3, cudaStream_t s, Hook hook) {
+    const int64_t n = 3 * N;
+    const int64_t np = pad_for(kind, n);
+    const int64_t Mp = compact_Mp(M), Kc = compact_Kc(cap);
+    const size_t esz = esz_of(kind);
+    FCB_TRY(h->sp_coef.ensure(sizeof(float) * (size_t)N * 27 * 3 * cap));
+    FCB_TRY(lj_sparse_coefs(h, N, tol, d_m, d_nb, d_count, d_self, cap, h->sp_coef.as<float>(), s));
+    phase_mark(h, s, 3);
+    FCB_TRY(h->u1_hi.ensure(esz * Mp * n * Kc));
+    FCB_TRY(h->u1_lo.ensure(esz * Mp * n * Kc));
+    FCB_TRY(h->phik_hi.ensure(esz * N * M * Kc));
+    FCB_TRY(h->phik_lo.ensure(esz * N * M * Kc));
+    FCB_TRY(sparse_p1c_launch(kind, N, cap, d_nb, d_count, d_self, h->sp_coef.as<float>(), d_phi, mode_lo, M, Mp, Kc,
+                              h->u1_hi.p, h->u1_lo.p, h->phik_hi.p, h->phik_lo.p, s));
+    phase_mark(h, s, 4);
+    FCB_TRY(h->u2_hi.ensure(esz * Mp * n * M));
+    FCB_TRY(h->u2_lo.ensure(esz * Mp * n * M));
+    ModeProduct p2{Mp * n, Kc, M, Kc, Kc, Mp, Mp, Mp * n};
+    p2.sym_inner = true;
+    p2.b_group = 3 * Mp;
+    p2.b_group_ld = M;
+    FCB_TRY(mode_product_tc(h, kind, h->u1_hi.p, h->u1_lo.p, h->phik_hi.p, h->phik_lo.p, h->u2_hi.p, h->u2_lo.p, kind,
+                            p2, s));
+    phase_mark(h, s, 5);
+    FCB_TRY(hook());
+    const size_t poff = esz * np * mode_lo;
+    ModeProduct p3{Mp * M, n, M, Mp, np, Mp, M, M * M};
+    p3.sym = true;
+    p3.a_mn = true;
+    p3.lda_z = Mp * n;
+    p3.Fv = M;
+    return mode_product_tc(h, kind, h->u2_hi.p, h->u2_lo.p, static_cast<const uint8_t*>(h->phi_hi.p) + poff,
+                           static_cast<const uint8_t*>(h->phi_lo.p) + poff, d_k3, nullptr, 0, p3, s);
+}
+
+// The compact form where it applies, else the dense-layout sparse form; the
+// hook runs once, before the third product or after the first.
+template <class Hook>
+int sparse_snapshot_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, int kind, int cap,
+                             const int* d_nb, const int* d_count, const int* d_self, double tol, const double* d_m,
+                             const float* d_phi, float* d_k3, cudaStream_t s, Hook hook) {
+    if (tc_pair_enabled() && compact_pays(3 * N, M, cap))
+        return compact_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s, hook);
+    return sparse_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s, hook);
+}
+
 // The LJ snapshot with a block-sparse first mode product (split precisions).
 // Needs the largest neighbour count on the host to size the coefficient
 // tables, so it synchronises the stream once (after the neighbour lists; the
 // φ split is already queued behind them).  The FP64 Ψ writer (HBM-bound) runs
-// on the aux stream beside P2 and P3 (tensor-core bound), with two blocks per
-// SM so that both kernels stay resident on every SM; the caller's stream waits
+// on the aux stream beside the tensor-core bound products (the third one in
+// the compact form, the second and third otherwise), with two blocks per SM
+// so that both kernels stay resident on every SM; the caller's stream waits
 // for it before the end (with phase timing on it runs alone instead, before
 // the sparse products).  Sets *used = false, having done nothing visible, when
 // the neighbourhoods are so large that the sparse form does not pay; the
@@ -743,8 +798,8 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
         writer = true;
         return FCB_OK;
     };
-    const int rc = sparse_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s,
-                                   launch_writer);
+    const int rc = sparse_snapshot_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi,
+                                            d_k3, s, launch_writer);
     if (writer) FCB_CUDA(cudaStreamWaitEvent(s, h->ev[3], 0));
     FCB_TRY(rc);
     phase_mark(h, s, 6);
@@ -791,8 +846,8 @@ int snapshot_lj_sparse_device(fcb200_context* h, const double* d_pos, int64_t N,
     FCB_TRY(lj_neighbour_lists(h, N, d_nb, d_count, d_self, d_max, s));
     FCB_TRY(split_phi(h, kind, d_phi, 3 * N, s));
     phase_mark(h, s, 2);
-    FCB_TRY(sparse_products(h, N, mode_lo, mode_hi - mode_lo, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi,
-                            d_k3, s, [] { return (int)FCB_OK; }));
+    FCB_TRY(sparse_snapshot_products(h, N, mode_lo, mode_hi - mode_lo, kind, cap, d_nb, d_count, d_self, tol, d_m,
+                                     d_phi, d_k3, s, [] { return (int)FCB_OK; }));
     phase_mark(h, s, 6);
     return FCB_OK;
 }

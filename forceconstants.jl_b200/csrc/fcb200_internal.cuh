@@ -84,6 +84,7 @@ struct fcb200_context {
     fcb::Buf adj_phiT, adj_w_hi, adj_w_lo, adj_pairs, adj_G, adj_scal, adj_w32, adj_dpos;
     // block-sparse P1 of the LJ snapshot: neighbour lists and coefficient tables
     fcb::Buf sp_ints, sp_coef;
+    fcb::Buf phik_hi, phik_lo;      // compact sparse form: per-atom φ rows (split)
     // finite differences: staged element list and output
     fcb::Buf fd_elems, fd_out;
     // get_modes: eigensolver handle (cusolverDnHandle_t, opened on first use) and scratch
@@ -191,6 +192,22 @@ struct ModeProduct {
     // their rows' outer index are skipped and every computed entry with
     // column > outer index is also stored mirrored.  Needs R = F·M rows.
     bool sym = false;
+    // The forms below run on the 2-CTA tensor-core tile only, with R a
+    // multiple of 256 and F, F_pad, ldd, Fv and M multiples of 8.
+    // Output symmetric under exchanging the row's inner index (r % F) and the
+    // column, inside each outer block (U2[k,p,q] = U2[k,q,p] with rows p + F·k):
+    // tiles wholly below the diagonal are skipped and tiles wholly above it are
+    // also stored transposed.  F a multiple of 256; mode tiles 256 wide.
+    bool sym_inner = false;
+    // A read MN-major: A[r,a] at (r % F) + lda·a + lda_z·(r / F); F a multiple
+    // of 128 and R of F.
+    bool a_mn = false;
+    int64_t lda_z = 0;
+    // Grouped B: rows [g·b_group, (g+1)·b_group) of A use B[a + ldb·(p + b_group_ld·g)]
+    // (0 = one B for all rows); b_group a multiple of 256.
+    int64_t b_group = 0, b_group_ld = 0;
+    // Rows with r % F >= Fv are computed but not stored (0 = F).
+    int64_t Fv = 0;
 };
 
 int mode_product_f32(const float* A, const float* B, float* D, const ModeProduct& mp,
@@ -208,6 +225,27 @@ int lj_neighbour_lists(fcb200_context* h, int64_t N, int* d_nb, int* d_count, in
 int lj_sparse_coefs(fcb200_context* h, int64_t N, double tol, const double* d_masses, const int* d_nb,
                     const int* d_count, const int* d_self, int cap, float* d_coef, cudaStream_t s);
 size_t sparse_p1_smem_bytes(int cap, int64_t N);
+// Compact first product (sparse_mcc3.cu): U1c[j' + Kc·(p + Mp·k)] and the
+// per-atom φ rows φK[j' + Kc·(q + M·K)], split into hi/lo planes of `kind`.
+size_t sparse_p1c_smem_bytes(int cap);
+int sparse_p1c_launch(int kind, int64_t N, int cap, const int* d_nb, const int* d_count, const int* d_self,
+                      const float* d_coef, const float* d_phi, int64_t mode_lo, int64_t M, int64_t Mp, int64_t Kc,
+                      void* u1_hi, void* u1_lo, void* pk_hi, void* pk_lo, cudaStream_t s);
+// Whether mode products run on the 2-CTA tile (mode_product_tc.cu).
+bool tc_pair_enabled();
+// Shapes of the compact sparse products: modes padded to whole 256-row blocks,
+// neighbourhood rows to a multiple of 8.
+inline int64_t compact_Mp(int64_t M) { return (M + 255) / 256 * 256; }
+inline int64_t compact_Kc(int cap) { return (3 * (int64_t)cap + 7) / 8 * 8; }
+// The compact form pays when its grouped second product and padded third
+// product execute at least 10 % fewer tile flops than the dense-K pair.
+inline bool compact_pays(int64_t n, int64_t M, int cap) {
+    if (M % 8 != 0) return false;
+    const double Mp = (double)compact_Mp(M), Kc = (double)compact_Kc(cap);
+    const double compact = Mp * n * Kc + Mp * M * n;
+    const double dense = (double)n * M * n + (double)M * M * n;
+    return compact < 0.9 * dense;
+}
 int sparse_p1_launch(fcb200_context* h, int kind, int64_t N, int cap, const int* d_nb, const int* d_count,
                      const int* d_self, const float* d_coef, const float* d_phi, int64_t np, int64_t mode_lo,
                      int64_t M, void* u1_hi, void* u1_lo, cudaStream_t s);

@@ -52,8 +52,11 @@ struct TcParams {
     int64_t F, F_pad, ldd;
     int bn, n_tiles, m_tiles, k_chunks, elems_per_row;
     int out_kind;
-    int sym;  // symmetric output (pair kernel): see ModeProduct::sym
+    int sym;  // symmetric output (pair kernel): 1 = ModeProduct::sym, 2 = ModeProduct::sym_inner
     int vec;  // F, F_pad, ldd multiples of 8: 8 consecutive rows are 8 consecutive, aligned elements
+    int a_mn;                      // A read MN-major through a 3-D map (ModeProduct::a_mn)
+    int64_t b_group, b_group_ld;   // ModeProduct::b_group / b_group_ld (pair kernel)
+    int64_t Fv;                    // rows r with r % F >= Fv are not stored
     void* d_hi;
     void* d_lo;
     int* status;
@@ -140,11 +143,32 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     return d;
 }
 
-// Instruction descriptor: FP32 accumulator, both operands K-major.
+// Shared-memory matrix descriptor: MN-major.  Each 128-byte row holds
+// consecutive M (or N) elements of one K index, and the atoms of the next 128
+// bytes of M lie `lbo` bytes further on.  BF16: 128-byte swizzle of 16-byte
+// chunks, 8-row K groups 1024 bytes apart.  TF32: MN-major 32-bit operands take
+// the 128-byte swizzle of 32-byte chunks (layout type 1), 4-row K groups 512
+// bytes apart.
 template <int KIND>
-__device__ __forceinline__ uint32_t instr_desc(int m, int n) {
+__device__ __forceinline__ uint64_t smem_desc_mn(uint32_t addr, uint32_t lbo) {
+    constexpr uint32_t sbo = KIND == 1 ? 1024u : 512u;
+    constexpr uint64_t layout = KIND == 1 ? 2u : 1u;
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;  // leading byte offset: between 128-byte M atoms
+    d |= (uint64_t)(sbo >> 4) << 32;             // stride byte offset: between K groups
+    d |= (uint64_t)1 << 46;                      // descriptor version for tcgen05
+    d |= layout << 61;
+    return d;
+}
+
+// Instruction descriptor: FP32 accumulator, B K-major, A K-major or (a_mn)
+// MN-major.
+template <int KIND>
+__device__ __forceinline__ uint32_t instr_desc(int m, int n, bool a_mn = false) {
     const uint32_t fmt = KIND == 1 ? 1u : 2u;  // BF16 : TF32
-    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((a_mn ? 1u : 0u) << 15) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(m >> 4) << 24);
 }
 
 template <int KIND>
@@ -273,9 +297,11 @@ __device__ __forceinline__ void store_vec8(const TcParams& p, int64_t off, const
     }
 }
 
-// Symmetric output: does pair tile (mt, nt) hold any column >= its rows' outer index?
+// Symmetric output: does pair tile (mt, nt) hold any column >= its rows' outer
+// index (sym 1), or any column >= its rows' inner index (sym 2: the 256 rows of
+// a tile share one outer index and the tiles are square)?
 __device__ __forceinline__ bool sym_tile_live(const TcParams& p, int mt, int nt) {
-    const int64_t pmin = ((int64_t)mt * 256) / p.F;
+    const int64_t pmin = p.sym == 2 ? ((int64_t)mt * 256) % p.F : ((int64_t)mt * 256) / p.F;
     int64_t qmax = (int64_t)nt * p.bn + p.bn;
     if (qmax > p.M) qmax = p.M;
     return qmax - 1 >= pmin;
@@ -501,6 +527,15 @@ __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* m
         : "memory");
 }
 
+__device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* map, uint32_t bar_cluster, int x,
+                                                 int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+        "%3, %4}], [%5];" ::"r"(saddr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar_cluster)
+        : "memory");
+}
+
 template <int KIND>
 __device__ __forceinline__ void umma_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     if constexpr (KIND == 1) {
@@ -601,10 +636,23 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     const uint32_t fb = mapa_shared(saddr(&full[stage]), 0);
                     if (leader) mbar_expect_tx(&full[stage], tx_pair);
                     const int x = kc * p.elems_per_row;
-                    tma_load_2d_pair(st, &mA_hi, fb, x, mt * 256 + (int)rank * 128);
-                    tma_load_2d_pair(st + A_BYTES, &mA_lo, fb, x, mt * 256 + (int)rank * 128);
-                    tma_load_2d_pair(st + 2 * A_BYTES, &mB_hi, fb, x, nt * p.bn + (int)rank * half);
-                    tma_load_2d_pair(st + 2 * A_BYTES + B2_BYTES, &mB_lo, fb, x, nt * p.bn + (int)rank * half);
+                    const int64_t row0 = (int64_t)mt * 256 + (int)rank * 128;
+                    if (p.a_mn) {
+                        // 128 rows = (128 / epr) boxes of epr M-elements × epr K-rows
+                        const int z = (int)(row0 / p.F), m0 = (int)(row0 % p.F);
+                        for (int i = 0; i < 128 / p.elems_per_row; ++i) {
+                            const int off = i * p.elems_per_row * ROW_BYTES;
+                            tma_load_3d_pair(st + off, &mA_hi, fb, m0 + i * p.elems_per_row, x, z);
+                            tma_load_3d_pair(st + A_BYTES + off, &mA_lo, fb, m0 + i * p.elems_per_row, x, z);
+                        }
+                    } else {
+                        tma_load_2d_pair(st, &mA_hi, fb, x, (int)row0);
+                        tma_load_2d_pair(st + A_BYTES, &mA_lo, fb, x, (int)row0);
+                    }
+                    const int by = nt * p.bn + (int)rank * half +
+                                   (p.b_group ? (int)(((int64_t)mt * 256 / p.b_group) * p.b_group_ld) : 0);
+                    tma_load_2d_pair(st + 2 * A_BYTES, &mB_hi, fb, x, by);
+                    tma_load_2d_pair(st + 2 * A_BYTES + B2_BYTES, &mB_lo, fb, x, by);
                     filled |= 1u << stage;
                     filled_phase = (filled_phase & ~(1u << stage)) | (phase << stage);
                     if (++stage == STAGES2) stage = 0, phase ^= 1;
@@ -621,7 +669,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     } else if (warp == 1) {
         if (lane == 0 && leader) {
             // ------------------------------------------------ MMA issuer (leader)
-            const uint32_t idesc = instr_desc<KIND>(256, p.bn);
+            const uint32_t idesc = instr_desc<KIND>(256, p.bn, p.a_mn != 0);
+            // MN-major A: one UMMA K step (32 bytes of K) is 32/esz K-rows of 128 bytes
+            const uint32_t a_step = p.a_mn ? (uint32_t)(32 / (KIND == 1 ? 2 : 4)) * ROW_BYTES : 32u;
+            const uint32_t a_lbo = (uint32_t)p.elems_per_row * ROW_BYTES;
             int stage = 0, acc = 0;
             uint32_t phase = 0, acc_phase = 0;
             bool ok = true, issued = false;
@@ -640,15 +691,18 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     }
                     tc_fence_after();
                     const uint32_t base = saddr(smem + stage * STAGE2_BYTES);
-                    const uint64_t a_hi = smem_desc(base), a_lo = smem_desc(base + A_BYTES);
+                    const uint64_t a_hi = p.a_mn ? smem_desc_mn<KIND>(base, a_lbo) : smem_desc(base);
+                    const uint64_t a_lo =
+                        p.a_mn ? smem_desc_mn<KIND>(base + A_BYTES, a_lbo) : smem_desc(base + A_BYTES);
                     const uint64_t b_hi = smem_desc(base + 2 * A_BYTES);
                     const uint64_t b_lo = smem_desc(base + 2 * A_BYTES + B2_BYTES);
 #pragma unroll
                     for (int k = 0; k < ROW_BYTES / 32; ++k) {
                         const uint64_t off = (uint64_t)((k * 32) >> 4);
-                        umma_pair<KIND>(d_tmem, a_hi + off, b_hi + off, idesc, (kc | k) != 0);
-                        umma_pair<KIND>(d_tmem, a_hi + off, b_lo + off, idesc, 1u);
-                        umma_pair<KIND>(d_tmem, a_lo + off, b_hi + off, idesc, 1u);
+                        const uint64_t aoff = (uint64_t)((k * a_step) >> 4);
+                        umma_pair<KIND>(d_tmem, a_hi + aoff, b_hi + off, idesc, (kc | k) != 0);
+                        umma_pair<KIND>(d_tmem, a_hi + aoff, b_lo + off, idesc, 1u);
+                        umma_pair<KIND>(d_tmem, a_lo + aoff, b_hi + off, idesc, 1u);
                     }
                     umma_commit_pair_both(&empty[stage]);
                     issued = true;
@@ -679,11 +733,13 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             if (!ok) break;
             tc_fence_after();
             const int64_t row = (int64_t)mt * 256 + rank * 128 + q * 32 + lane;
-            const bool row_ok = row < p.R;
+            const bool row_ok = row < p.R && (row % p.F) < p.Fv;
             const int64_t row_off = row_ok ? (row % p.F) + p.F_pad * (row / p.F) : 0;
             const int64_t col0 = (int64_t)nt * p.bn;
             const int64_t wrow0 = (int64_t)mt * 256 + rank * 128 + q * 32;  // the warp's first row
             const bool warp_vec = p.vec && wrow0 + 32 <= p.R;
+            // sym 2: a tile wholly above the diagonal is also stored transposed
+            const bool sym2_mirror = p.sym == 2 && (int64_t)nt * p.bn >= ((int64_t)mt * 256) % p.F + 256;
             float* stg = stage_base + (warp - 2) * (32 * STG_LD);
             for (int ch = 0; ch < chunks; ++ch) {
                 uint32_t v[32];
@@ -701,16 +757,33 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     const int m = lane & 3;
                     const int64_t r0 = wrow0 + 8 * m;
                     const int64_t pr = r0 / p.F, kr = r0 - pr * p.F;
+                    const bool kr_ok = kr < p.Fv;  // 8-row groups are all valid or all not (Fv % 8 == 0)
 #pragma unroll
                     for (int rd = 0; rd < 4; ++rd) {
                         const int j = 8 * rd + (lane >> 2);
-                        if (j >= ncols) continue;
+                        if (j >= ncols || !kr_ok) continue;
                         const float4 a = *reinterpret_cast<const float4*>(stg + j * STG_LD + 8 * m);
                         const float4 b = *reinterpret_cast<const float4*>(stg + j * STG_LD + 8 * m + 4);
                         const float x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
                         const int64_t qq = c0 + j;
-                        if (!p.sym || qq >= pr) store_vec8(p, kr + p.F_pad * pr + p.ldd * qq, x);
-                        if (p.sym && qq > pr) store_vec8(p, kr + p.F_pad * qq + p.ldd * pr, x);
+                        if (p.sym != 1 || qq >= pr) store_vec8(p, kr + p.F_pad * pr + p.ldd * qq, x);
+                        if (p.sym == 1 && qq > pr) store_vec8(p, kr + p.F_pad * qq + p.ldd * pr, x);
+                    }
+                    if (sym2_mirror) {
+                        // (k, q, p) for the tile above the diagonal: 8 consecutive
+                        // columns of this lane's row per 16-byte store
+                        const int64_t rr = wrow0 + lane;
+                        const int64_t pk = rr / p.F, pp = rr - pk * p.F;
+                        if (pp < p.M) {
+#pragma unroll
+                            for (int g = 0; g < 4; ++g) {
+                                if (8 * g >= ncols) break;
+                                float x[8];
+#pragma unroll
+                                for (int i = 0; i < 8; ++i) x[i] = stg[(8 * g + i) * STG_LD + lane];
+                                store_vec8(p, (c0 + 8 * g) + p.F_pad * pk + p.ldd * pp, x);
+                            }
+                        }
                     }
                     __syncwarp();
                     continue;
@@ -791,6 +864,29 @@ int make_map(CUtensorMap* m, const void* base, int kind, int64_t K, int64_t rows
     return FCB_OK;
 }
 
+// 3-D map of an MN-major operand: element (m, k, z) at m + ld1·k + ld2·z; box
+// of 128 bytes of m × epr k-rows × 1, swizzled as the MN-major descriptor of
+// the kind expects (16-byte chunks for BF16, 32-byte chunks for TF32).
+int make_map_mn(CUtensorMap* m, const void* base, int kind, int64_t Mx, int64_t K, int64_t Z, int64_t ld1,
+                int64_t ld2) {
+    EncodeFn enc = encode_fn();
+    if (!enc) return set_error(FCB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const int esz = kind == 1 ? 2 : 4;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (ld1 * esz) % 16 != 0 || (ld2 * esz) % 16 != 0)
+        return set_error(FCB_ERR_ARG, "MN-major operand is not 16-byte aligned");
+    const cuuint32_t epr = (cuuint32_t)(ROW_BYTES / esz);
+    cuuint64_t dims[3] = {(cuuint64_t)Mx, (cuuint64_t)K, (cuuint64_t)Z};
+    cuuint64_t strides[2] = {(cuuint64_t)(ld1 * esz), (cuuint64_t)(ld2 * esz)};
+    cuuint32_t box[3] = {epr, epr, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(m, kind == 1 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                     const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     kind == 1 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(FCB_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return FCB_OK;
+}
+
 }  // namespace
 
 // The 2-CTA tile is the default; FCB200_TC_PAIR=0 selects the 1-CTA tile.
@@ -802,6 +898,8 @@ static bool use_pair_kernel() {
     }
     return v == 1;
 }
+
+bool tc_pair_enabled() { return use_pair_kernel(); }
 
 int pad_for(int kind, int64_t n) {
     // TMA needs 16-byte row strides: 8 BF16 or 4 FP32 elements.
@@ -855,16 +953,35 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
     p.F = mp.F;
     p.F_pad = mp.F_pad;
     p.ldd = mp.ldd;
-    p.sym = mp.sym ? 1 : 0;
+    p.sym = mp.sym_inner ? 2 : mp.sym ? 1 : 0;
     p.vec = (mp.F % 8 == 0 && mp.F_pad % 8 == 0 && mp.ldd % 8 == 0) ? 1 : 0;
+    p.a_mn = mp.a_mn ? 1 : 0;
+    p.b_group = mp.b_group;
+    p.b_group_ld = mp.b_group_ld;
+    p.Fv = mp.Fv > 0 ? mp.Fv : mp.F;
     if (mp.sym && mp.R != mp.F * mp.M) return set_error(FCB_ERR_ARG, "mode_product_tc: symmetric output needs R = F*M");
+    const bool ext = mp.sym_inner || mp.a_mn || mp.b_group || p.Fv != mp.F;
+    if (ext) {
+        // forms of the 2-CTA kernel only; every warp takes the 16-byte store path
+        if (!(use_pair_kernel() && h->sm_count >= 2))
+            return set_error(FCB_ERR_UNSUPPORTED, "mode_product_tc: grouped / MN-major forms need the 2-CTA tile");
+        if (!p.vec || mp.R % 256 != 0 || p.Fv % 8 != 0 || mp.M % 8 != 0)
+            return set_error(FCB_ERR_ARG, "mode_product_tc: grouped / MN-major forms need 8-aligned shapes");
+        if (mp.sym_inner && (mp.sym || mp.F % 256 != 0))
+            return set_error(FCB_ERR_ARG, "mode_product_tc: inner symmetry needs 256-row blocks");
+        if (mp.a_mn && (mp.F % 128 != 0 || mp.R % mp.F != 0))
+            return set_error(FCB_ERR_ARG, "mode_product_tc: MN-major A needs 128-row blocks");
+        if (mp.b_group && mp.b_group % 256 != 0)
+            return set_error(FCB_ERR_ARG, "mode_product_tc: B groups must hold whole 256-row tiles");
+    }
     p.n_tiles = (int)((mp.M + BN_MAX - 1) / BN_MAX);
-    if (h->tune) {  // autotuned mode-tile count for this shape, if any
+    if (h->tune && !mp.sym_inner) {  // autotuned mode-tile count for this shape, if any
         auto it = h->tune->find(tune_key(kind, mp.R, mp.K, mp.M));
         if (it != h->tune->end() && it->second >= p.n_tiles && it->second <= mp.M) p.n_tiles = it->second;
     }
     const int64_t per = (mp.M + p.n_tiles - 1) / p.n_tiles;
     p.bn = (int)(((per + 15) / 16) * 16);
+    if (mp.sym_inner && mp.M > 256) p.bn = 256;  // square 256 × 256 tiles
     p.m_tiles = (int)((mp.R + BM - 1) / BM);
     p.elems_per_row = ROW_BYTES / (kind == 1 ? 2 : 4);
     p.k_chunks = (int)((mp.K + p.elems_per_row - 1) / p.elems_per_row);
@@ -873,16 +990,23 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
     p.d_lo = D_lo;
     p.status = h->d_status;
     CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
-    FCB_TRY(make_map(&ma_hi, A_hi, kind, mp.K, mp.R, mp.lda, BM));
-    FCB_TRY(make_map(&ma_lo, A_lo, kind, mp.K, mp.R, mp.lda, BM));
-    FCB_TRY(make_map(&mb_hi, B_hi, kind, mp.K, mp.M, mp.ldb, p.bn));
-    FCB_TRY(make_map(&mb_lo, B_lo, kind, mp.K, mp.M, mp.ldb, p.bn));
+    // B rows: the modes, or (grouped) every group's modes one after another
+    const int64_t b_rows = mp.b_group ? mp.b_group_ld * ((mp.R + mp.b_group - 1) / mp.b_group) : mp.M;
+    if (mp.a_mn) {
+        FCB_TRY(make_map_mn(&ma_hi, A_hi, kind, mp.F, mp.K, mp.R / mp.F, mp.lda, mp.lda_z));
+        FCB_TRY(make_map_mn(&ma_lo, A_lo, kind, mp.F, mp.K, mp.R / mp.F, mp.lda, mp.lda_z));
+    } else {
+        FCB_TRY(make_map(&ma_hi, A_hi, kind, mp.K, mp.R, mp.lda, BM));
+        FCB_TRY(make_map(&ma_lo, A_lo, kind, mp.K, mp.R, mp.lda, BM));
+    }
+    FCB_TRY(make_map(&mb_hi, B_hi, kind, mp.K, b_rows, mp.ldb, p.bn));
+    FCB_TRY(make_map(&mb_lo, B_lo, kind, mp.K, b_rows, mp.ldb, p.bn));
     if (use_pair_kernel() && h->sm_count >= 2) {
         // 2-CTA tiles: 256 rows per pair, each CTA loads half of the mode tile
         p.m_tiles = (int)((mp.R + 255) / 256);
         CUtensorMap pb_hi, pb_lo;
-        FCB_TRY(make_map(&pb_hi, B_hi, kind, mp.K, mp.M, mp.ldb, p.bn / 2));
-        FCB_TRY(make_map(&pb_lo, B_lo, kind, mp.K, mp.M, mp.ldb, p.bn / 2));
+        FCB_TRY(make_map(&pb_hi, B_hi, kind, mp.K, b_rows, mp.ldb, p.bn / 2));
+        FCB_TRY(make_map(&pb_lo, B_lo, kind, mp.K, b_rows, mp.ldb, p.bn / 2));
         const int64_t tiles2 = (int64_t)p.m_tiles * p.n_tiles;
         if (kind == 1) return launch_pair(mode_product_tc2_kernel<1>, 1, h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
         return launch_pair(mode_product_tc2_kernel<2>, 2, h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);

@@ -23,6 +23,7 @@ namespace {
 constexpr int PC = 32;  // modes per CTA
 constexpr int PB = 4;   // modes per shared-memory column block
 constexpr int CJ = 8;   // rows per 16-byte store of a BF16 plane
+constexpr int P1C_THREADS = 384;  // compact form: ≥ 3·Kc/2 tasks for neighbourhoods up to 84 atoms
 
 struct SparseP1Args {
     int N, n, cap, M, mode_lo;
@@ -213,6 +214,138 @@ __global__ void __launch_bounds__(256) sparse_p1_kernel(SparseP1Args a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Compact first product.  U1[j,k,p] vanishes unless j ∈ nbr(atom(k)), so the
+// compact form keeps, for every column k = 3K + kc and mode p, only the rows
+// of K's neighbourhood in slot order:
+//     U1c[j' + Kc·(p + Mp·k)],  j' = 3·slot + jc < 3·|nbr(K)|, zero up to Kc,
+// and, as the second product's per-atom operand, the same rows of φ:
+//     φK[j' + Kc·(q + M·K)] = φ[3·nbr(K)[slot] + jc, q].
+// The second product is then a grouped GEMM over the atoms with Kc (about
+// 3·|nbr|) instead of n terms.  One CTA per (atom K, PC modes); one thread per
+// (kc, pair of rows j') walks the modes with its 12 coefficients in registers;
+// a warp stores 128 contiguous bytes per plane.  Rows p ≥ M (up to Mp) are
+// written as zeros.
+struct SparseP1cArgs {
+    int N, n, cap, M, Mp, Kc, mode_lo;
+    const int* nb;
+    const int* count;
+    const int* self_slot;
+    const float* coef;
+    const float* phi;
+    void* u1_hi;
+    void* u1_lo;
+    void* pk_hi;
+    void* pk_lo;
+};
+
+template <int KIND>
+__device__ __forceinline__ void store_pair(void* hi, void* lo, int64_t off, float v0, float v1) {
+    if constexpr (KIND == 1) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(v0 - __low2float(h), v1 - __high2float(h));
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(hi) + off) = h;
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(lo) + off) = l;
+    } else {
+        uint32_t b0, b1;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b0) : "f"(v0));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b1) : "f"(v1));
+        const float h0 = __uint_as_float(b0), h1 = __uint_as_float(b1);
+        *reinterpret_cast<float2*>(static_cast<float*>(hi) + off) = make_float2(h0, h1);
+        *reinterpret_cast<float2*>(static_cast<float*>(lo) + off) = make_float2(v0 - h0, v1 - h1);
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a) {
+    extern __shared__ float sm[];
+    const int K = blockIdx.y, p0 = blockIdx.x * PC;
+    const int L = 3 * a.cap;
+    const int cnt = a.count[K], ss = a.self_slot[K];
+    if (cnt > a.cap) return;  // reported by the coefficient kernel; the output is invalid
+    float* phis = sm;                       // [L][PC+1]
+    float* cp = phis + L * (PC + 1);        // pair part [3][6][L], then self part [3][3][L]
+    float* cs = cp + 18 * L;
+    float* selfres = cp + 27 * L;           // [9][PC]
+    const int* nbK = a.nb + (int64_t)K * a.N;
+    for (int il = threadIdx.x; il < L; il += blockDim.x) {
+        const int sl = il / 3;
+        const bool live = sl < cnt;
+        const int64_t src = live ? (int64_t)(3 * nbK[sl] + il % 3) + (int64_t)a.n * (a.mode_lo + p0) : 0;
+#pragma unroll 8
+        for (int pp = 0; pp < PC; ++pp)
+            phis[il * (PC + 1) + pp] = (live && p0 + pp < a.M) ? a.phi[src + (int64_t)a.n * pp] : 0.f;
+    }
+    {
+        const float4* cg = reinterpret_cast<const float4*>(a.coef + (int64_t)K * 27 * L);
+        float4* c4 = reinterpret_cast<float4*>(cp);
+        for (int e = threadIdx.x; e < 27 * L / 4; e += blockDim.x) c4[e] = cg[e];
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < 3 * PC; o += blockDim.x) {
+        const int pp = o % PC, g = o / PC;  // kj = g, g+3, g+6
+        const float* c0 = cs + g * L;
+        const float* c1 = cs + (g + 3) * L;
+        const float* c2 = cs + (g + 6) * L;
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+        for (int il = 0; il < 3 * cnt; ++il) {
+            const float ph = phis[il * (PC + 1) + pp];
+            s0 = fmaf(c0[il], ph, s0);
+            s1 = fmaf(c1[il], ph, s1);
+            s2 = fmaf(c2[il], ph, s2);
+        }
+        selfres[g * PC + pp] = s0;
+        selfres[(g + 3) * PC + pp] = s1;
+        selfres[(g + 6) * PC + pp] = s2;
+    }
+    // φK rows of this CTA's modes (no dependence on the self sums)
+    const int npair = a.Kc / 2;
+    for (int it = threadIdx.x; it < PC * npair; it += blockDim.x) {
+        const int pp = it / npair, j0 = 2 * (it - pp * npair);
+        if (p0 + pp >= a.M) break;
+        const float v0 = j0 < 3 * cnt ? phis[j0 * (PC + 1) + pp] : 0.f;
+        const float v1 = j0 + 1 < 3 * cnt ? phis[(j0 + 1) * (PC + 1) + pp] : 0.f;
+        store_pair<KIND>(a.pk_hi, a.pk_lo, (int64_t)j0 + (int64_t)a.Kc * ((p0 + pp) + (int64_t)a.M * K), v0, v1);
+    }
+    __syncthreads();
+    for (int task = threadIdx.x; task < 3 * npair; task += blockDim.x) {
+        const int kc = task / npair, j0 = 2 * (task - kc * npair);
+        float c[2][6];
+        int rowj[2];
+        bool self[2], valid[2];
+        const float* sres[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int jv = j0 + h, sl = jv / 3, jc = jv - 3 * sl;
+            valid[h] = sl < cnt;
+            self[h] = sl == ss;
+            const bool pair = valid[h] && !self[h];
+            rowj[h] = pair ? 3 * sl : 3 * ss;
+#pragma unroll
+            for (int t2 = 0; t2 < 6; ++t2) c[h][t2] = pair ? cp[(kc * 6 + t2) * L + jv] : 0.f;
+            sres[h] = selfres + (kc * 3 + jc) * PC;
+        }
+        const float* yk = phis + 3 * ss * (PC + 1);
+        int64_t off = (int64_t)j0 + (int64_t)a.Kc * (p0 + (int64_t)a.Mp * (3 * K + kc));
+        for (int pp = 0; pp < PC; ++pp, off += a.Kc) {
+            const float y0 = yk[pp], y1 = yk[(PC + 1) + pp], y2 = yk[2 * (PC + 1) + pp];
+            float v[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const float* xj = phis + rowj[h] * (PC + 1) + pp;
+                float s = c[h][0] * xj[0];
+                s = fmaf(c[h][1], xj[PC + 1], s);
+                s = fmaf(c[h][2], xj[2 * (PC + 1)], s);
+                s = fmaf(c[h][3], y0, s);
+                s = fmaf(c[h][4], y1, s);
+                s = fmaf(c[h][5], y2, s);
+                v[h] = !valid[h] ? 0.f : self[h] ? sres[h][pp] : s;
+            }
+            store_pair<KIND>(a.u1_hi, a.u1_lo, off, v[0], v[1]);
+        }
+    }
+}
+
 }  // namespace
 
 // cap must be a multiple of 4 (the coefficient tables are copied as float4).
@@ -248,6 +381,48 @@ int sparse_p1_launch(fcb200_context* h, int kind, int64_t N, int cap, const int*
     } else {
         FCB_CUDA(cudaFuncSetAttribute(sparse_p1_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         sparse_p1_kernel<2><<<grid, 256, smem, s>>>(a);
+    }
+    FCB_CUDA(cudaGetLastError());
+    return FCB_OK;
+}
+
+}  // namespace fcb
+
+namespace fcb {
+
+size_t sparse_p1c_smem_bytes(int cap) {
+    const size_t L = 3 * (size_t)cap;
+    return sizeof(float) * (L * (PC + 1) + 27 * L + 9 * PC);
+}
+
+int sparse_p1c_launch(int kind, int64_t N, int cap, const int* d_nb, const int* d_count, const int* d_self,
+                      const float* d_coef, const float* d_phi, int64_t mode_lo, int64_t M, int64_t Mp, int64_t Kc,
+                      void* u1_hi, void* u1_lo, void* pk_hi, void* pk_lo, cudaStream_t s) {
+    SparseP1cArgs a;
+    a.N = (int)N;
+    a.n = (int)(3 * N);
+    a.cap = cap;
+    a.M = (int)M;
+    a.Mp = (int)Mp;
+    a.Kc = (int)Kc;
+    a.mode_lo = (int)mode_lo;
+    a.nb = d_nb;
+    a.count = d_count;
+    a.self_slot = d_self;
+    a.coef = d_coef;
+    a.phi = d_phi;
+    a.u1_hi = u1_hi;
+    a.u1_lo = u1_lo;
+    a.pk_hi = pk_hi;
+    a.pk_lo = pk_lo;
+    const size_t smem = sparse_p1c_smem_bytes(cap);
+    const dim3 grid((unsigned)(Mp / PC), (unsigned)N);
+    if (kind == 1) {
+        FCB_CUDA(cudaFuncSetAttribute(sparse_p1c_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sparse_p1c_kernel<1><<<grid, P1C_THREADS, smem, s>>>(a);
+    } else {
+        FCB_CUDA(cudaFuncSetAttribute(sparse_p1c_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sparse_p1c_kernel<2><<<grid, P1C_THREADS, smem, s>>>(a);
     }
     FCB_CUDA(cudaGetLastError());
     return FCB_OK;

@@ -70,11 +70,37 @@ def test_sparse_mode_window_and_device_buffers(fcb, oracle, cuda_device, c324):
     assert mx <= TOL and rms <= TOL, (mx, rms)
 
 
-def test_sparse_snapshot_256_atoms(fcb, oracle, cuda_device):
-    s, pot, calc, psi64, psi_mw, phi = _case(fcb, oracle, (4, 4, 4), 0.05, 1234)
-    _, k3 = fcb.snapshot_lj(s, pot, calc, phi, precision="bf16x3")
-    ref = oracle.mcc3(psi_mw, phi.astype(np.float64))
+@pytest.fixture(scope="module")
+def c768(fcb, oracle):
+    case = _case(fcb, oracle, (4, 4, 4), 0.05, 1234)
+    return case + (oracle.mcc3(case[4], case[5].astype(np.float64)),)
+
+
+# 256 atoms take the compact form (neighbourhood-compact first product, grouped
+# second product, MN-major third product) in both split precisions.
+@pytest.mark.parametrize("precision", ["bf16x3", "tf32x3"])
+def test_sparse_snapshot_256_atoms(fcb, oracle, cuda_device, c768, precision):
+    s, pot, calc, psi64, psi_mw, phi, ref = c768
+    n = 3 * s.n_atoms
+    psi_out = np.empty((n, n, n), order="F")
+    _, k3 = fcb.snapshot_lj(s, pot, calc, phi, precision=precision, psi_out=psi_out)
     mx, rms = _err(k3, ref)
+    assert mx <= TOL and rms <= TOL, (mx, rms)
+    assert np.array_equal(psi_out, psi64)
+
+
+def test_compact_mode_window(fcb, oracle, cuda_device, c768):
+    # 304 modes: padded to 512 rows per block, a partial last 256-wide mode tile
+    import torch
+    from fcb200.arrays import julia_empty
+    s, pot, calc, psi64, psi_mw, phi, ref = c768
+    lo, hi = 8, 312
+    M = hi - lo
+    k3 = julia_empty((M, M, M), np.float32, "cuda")
+    fcb.snapshot_lj(s, pot, calc, torch.from_numpy(phi).to(cuda_device), precision="bf16x3", modes=(lo, hi),
+                    k3_out=k3)
+    torch.cuda.synchronize()
+    mx, rms = _err(k3.cpu().numpy(), ref[lo:hi, lo:hi, lo:hi])
     assert mx <= TOL and rms <= TOL, (mx, rms)
 
 
