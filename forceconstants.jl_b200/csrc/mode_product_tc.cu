@@ -307,6 +307,79 @@ __device__ __forceinline__ bool sym_tile_live(const TcParams& p, int mt, int nt)
     return qmax - 1 >= pmin;
 }
 
+// Transposed stores of one 32 × 32 block (inner symmetry): element (row r,
+// column c0 + j) goes to (c0 + j) + F_pad·(r / F) + ldd·(r % F), so the columns
+// of a row are contiguous.  Each lane packs its own row (v[j], j < 32) into the
+// warp's staging block — 16-byte chunks XOR-swizzled by row so that neither
+// the writes nor the reads conflict — and the warp then stores whole row
+// segments: 8 rows × 64 bytes (BF16) or 4 rows × 128 bytes (TF32, one plane
+// after the other) per instruction.  The output planes are of the operand
+// kind (the host requires out_kind == KIND with inner symmetry).  Rows whose inner index is not below M
+// (padding) and columns past `ncols` are not stored.
+// The warp's 32 rows lie in one block of F rows: outer index pk, inner indices
+// pp0 + row.
+template <int KIND>
+__device__ __forceinline__ void mirror_rows(const TcParams& p, uint8_t* sb, const uint32_t (&v)[32], int lane,
+                                            int64_t pk, int64_t pp0, int64_t c0, int64_t ncols) {
+    const int64_t base = c0 + p.F_pad * pk + p.ldd * pp0;
+    if constexpr (KIND == 1) {
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            uint32_t h[4], l[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const float a = __uint_as_float(v[8 * g + 2 * i]), b = __uint_as_float(v[8 * g + 2 * i + 1]);
+                const __nv_bfloat162 hb = __floats2bfloat162_rn(a, b);
+                const uint32_t hu = *reinterpret_cast<const uint32_t*>(&hb);
+                const __nv_bfloat162 lb =
+                    __floats2bfloat162_rn(a - __uint_as_float(hu << 16), b - __uint_as_float(hu & 0xFFFF0000u));
+                h[i] = hu;
+                l[i] = *reinterpret_cast<const uint32_t*>(&lb);
+            }
+            const int sw = g ^ ((lane >> 1) & 3);
+            *reinterpret_cast<uint4*>(sb + lane * 64 + sw * 16) = make_uint4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<uint4*>(sb + 2048 + lane * 64 + sw * 16) = make_uint4(l[0], l[1], l[2], l[3]);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int row = 8 * i + (lane >> 2), c = lane & 3, sw = c ^ ((row >> 1) & 3);
+            const uint4 vh = *reinterpret_cast<const uint4*>(sb + row * 64 + sw * 16);
+            const uint4 vl = *reinterpret_cast<const uint4*>(sb + 2048 + row * 64 + sw * 16);
+            if (pp0 + row < p.M && 8 * c < ncols) {
+                const int64_t off = base + 8 * c + p.ldd * row;
+                *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(p.d_hi) + off) = vh;
+                *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(p.d_lo) + off) = vl;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int plane = 0; plane < 2; ++plane) {
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+                float x[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float a = __uint_as_float(v[4 * g + i]), hv = tf32_round(a);
+                    x[i] = plane == 0 ? hv : a - hv;
+                }
+                const int sw = g ^ (lane & 7);
+                *reinterpret_cast<float4*>(sb + lane * 128 + sw * 16) = make_float4(x[0], x[1], x[2], x[3]);
+            }
+            __syncwarp();
+            float* dst = static_cast<float*>(plane == 0 ? p.d_hi : p.d_lo);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int row = 4 * i + (lane >> 3), c = lane & 7, sw = c ^ (row & 7);
+                const float4 y = *reinterpret_cast<const float4*>(sb + row * 128 + sw * 16);
+                if (pp0 + row < p.M && 4 * c < ncols)
+                    *reinterpret_cast<float4*>(dst + base + 4 * c + p.ldd * row) = y;
+            }
+            __syncwarp();
+        }
+    }
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     mode_product_tc_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant__ CUtensorMap mA_lo,
@@ -570,8 +643,11 @@ __device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
 }
 
+// 128 registers at most: the register file is split over the SM's four
+// partitions, and two 256-thread blocks of the FP64 Ψ writer (64 registers)
+// fit beside the pair kernel's six warps only at that size.
 template <int KIND>
-__global__ void __launch_bounds__(NUM_THREADS, 1)
+__global__ void __maxnreg__(128)
     mode_product_tc2_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant__ CUtensorMap mA_lo,
                             const __grid_constant__ CUtensorMap mB_hi, const __grid_constant__ CUtensorMap mB_lo,
                             const TcParams p) {
@@ -769,22 +845,6 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                         if (p.sym != 1 || qq >= pr) store_vec8(p, kr + p.F_pad * pr + p.ldd * qq, x);
                         if (p.sym == 1 && qq > pr) store_vec8(p, kr + p.F_pad * qq + p.ldd * pr, x);
                     }
-                    if (sym2_mirror) {
-                        // (k, q, p) for the tile above the diagonal: 8 consecutive
-                        // columns of this lane's row per 16-byte store
-                        const int64_t rr = wrow0 + lane;
-                        const int64_t pk = rr / p.F, pp = rr - pk * p.F;
-                        if (pp < p.M) {
-#pragma unroll
-                            for (int g = 0; g < 4; ++g) {
-                                if (8 * g >= ncols) break;
-                                float x[8];
-#pragma unroll
-                                for (int i = 0; i < 8; ++i) x[i] = stg[(8 * g + i) * STG_LD + lane];
-                                store_vec8(p, (c0 + 8 * g) + p.F_pad * pk + p.ldd * pp, x);
-                            }
-                        }
-                    }
                     __syncwarp();
                     continue;
                 }
@@ -814,6 +874,22 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
                         if (ch * 32 + j < p.bn && c0 + j < p.M) store_one(p, off + p.ldd * j, __uint_as_float(v[j]));
+                }
+            }
+            if (sym2_mirror && warp_vec) {
+                // the transposed copy, a second pass over the accumulator
+                // (kept apart from the direct stores to bound register use)
+                for (int ch = 0; ch < chunks; ++ch) {
+                    const int64_t c0 = col0 + ch * 32;
+                    int64_t ncols = p.M - c0;
+                    if (ncols > p.bn - ch * 32) ncols = p.bn - ch * 32;
+                    if (ncols > 32) ncols = 32;
+                    if (ncols <= 0) break;
+                    uint32_t v[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN_MAX + ch * 32), v);
+                    mirror_rows<KIND>(p, reinterpret_cast<uint8_t*>(stg), v, lane, wrow0 / p.F, wrow0 % p.F, c0,
+                                      ncols);
+                    __syncwarp();
                 }
             }
             tc_fence_before();
@@ -967,7 +1043,7 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
             return set_error(FCB_ERR_UNSUPPORTED, "mode_product_tc: grouped / MN-major forms need the 2-CTA tile");
         if (!p.vec || mp.R % 256 != 0 || p.Fv % 8 != 0 || mp.M % 8 != 0)
             return set_error(FCB_ERR_ARG, "mode_product_tc: grouped / MN-major forms need 8-aligned shapes");
-        if (mp.sym_inner && (mp.sym || mp.F % 256 != 0))
+        if (mp.sym_inner && (mp.sym || mp.F % 256 != 0 || out_kind != kind))
             return set_error(FCB_ERR_ARG, "mode_product_tc: inner symmetry needs 256-row blocks");
         if (mp.a_mn && (mp.F % 128 != 0 || mp.R % mp.F != 0))
             return set_error(FCB_ERR_ARG, "mode_product_tc: MN-major A needs 128-row blocks");
