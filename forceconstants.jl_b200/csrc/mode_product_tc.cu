@@ -13,12 +13,14 @@
 //   kind 2: TF32 values in FP32 planes, tcgen05.mma.kind::tf32  (TF32×3)
 // and each K step issues hi·hi + hi·lo + lo·hi into one FP32 TMEM accumulator.
 //
-// Kernel structure (persistent, one CTA per SM, 192 threads):
+// Kernel structure (persistent, one CTA per SM; 192 threads in the 1-CTA tile,
+// 192 or 320 in the CTA-pair tile, whose eight epilogue warps, where used, take
+// the even and odd 32-column chunks of each TMEM lane quadrant):
 //   warp 0      TMA producer: 4 tiled loads per stage (A_hi, A_lo, B_hi, B_lo),
 //               128-byte swizzle, no multicast, completion on an mbarrier.
 //   warp 1      TMEM allocation (512 columns = two 128×256 FP32 accumulators)
 //               and the single MMA-issuing thread.
-//   warps 2..5  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM lanes
+//   warps 2..5  (2..9) epilogue: tcgen05.ld of the accumulator (warp w reads TMEM lanes
 //               32*(w%4)..+31), conversion to the output format (FP32, or the
 //               hi/lo planes of the next product) and coalesced stores.
 // Double-buffered accumulators let the epilogue of tile t overlap the MMAs of
@@ -569,11 +571,22 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 constexpr int STAGES2 = 3;
 constexpr int B2_BYTES = (BN_MAX / 2) * ROW_BYTES;       // half of the mode tile, one plane
 constexpr int STAGE2_BYTES = 2 * A_BYTES + 2 * B2_BYTES;
-// Epilogue staging: per epilogue warp a 32-column × 32-row FP32 block, column
-// stride 36 floats (16-byte aligned rows, conflict-free 128-bit reads).
-constexpr int STG_LD = 36;
-constexpr int STG_BYTES = 4 * 32 * STG_LD * 4;
-constexpr int SMEM2_BYTES = STAGES2 * STAGE2_BYTES + 1024 + 256 + STG_BYTES;
+// Epilogue warps after the TMA-producer and MMA-issuer warps: 4 (one per TMEM
+// lane quadrant) or 8 (two per quadrant, even and odd 32-column chunks).  The
+// grouped second product, whose K is short, takes 8; the others take 4, which
+// leaves room on every SM for the FP64 Ψ writer running beside them.
+template <int EPI>
+constexpr int pair_threads() { return 32 * (2 + EPI); }
+// Epilogue staging: per epilogue warp a 32-column × 32-row FP32 block stored by
+// column (rows contiguous); the two 16-byte halves of every 8-row group swap
+// places in odd columns, so that the writes by row and the 128-bit reads by
+// column are both free of bank conflicts.
+constexpr int STG_LD = 32;
+template <int EPI>
+constexpr int pair_smem_bytes() { return STAGES2 * STAGE2_BYTES + 1024 + 256 + EPI * 32 * STG_LD * 4; }
+static_assert(pair_smem_bytes<8>() <= 232448, "pair-kernel shared memory over the 227 KB limit");
+
+__device__ __forceinline__ int stg_idx(int col, int row) { return col * STG_LD + (row ^ ((col & 1) << 2)); }
 
 __device__ __forceinline__ uint32_t cluster_rank() {
     uint32_t r;
@@ -645,8 +658,8 @@ __device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
 
 // 128 registers at most: the register file is split over the SM's four
 // partitions, and two 256-thread blocks of the FP64 Ψ writer (64 registers)
-// fit beside the pair kernel's six warps only at that size.
-template <int KIND>
+// fit beside the six warps of the 4-epilogue-warp form only at that size.
+template <int KIND, int EPI>
 __global__ void __maxnreg__(128)
     mode_product_tc2_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant__ CUtensorMap mA_lo,
                             const __grid_constant__ CUtensorMap mB_hi, const __grid_constant__ CUtensorMap mB_lo,
@@ -673,7 +686,7 @@ __global__ void __maxnreg__(128)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 8);  // 4 epilogue warps in each CTA
+            mbar_init(&tempty[b], 2 * EPI);  // the epilogue warps of both CTAs
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
@@ -796,7 +809,8 @@ __global__ void __maxnreg__(128)
         __syncwarp();
     } else {
         // ---------------------------------------------------- epilogue (both CTAs)
-        const int q = warp & 3;
+        const int q = warp & 3;             // TMEM lane quadrant this warp may access
+        const int cpar = (warp - 2) >> 2;   // with 8 epilogue warps: even (0) or odd (1) 32-column chunks
         int acc = 0;
         uint32_t acc_phase = 0;
         const int chunks = (p.bn + 31) / 32;
@@ -817,7 +831,7 @@ __global__ void __maxnreg__(128)
             // sym 2: a tile wholly above the diagonal is also stored transposed
             const bool sym2_mirror = p.sym == 2 && (int64_t)nt * p.bn >= ((int64_t)mt * 256) % p.F + 256;
             float* stg = stage_base + (warp - 2) * (32 * STG_LD);
-            for (int ch = 0; ch < chunks; ++ch) {
+            for (int ch = cpar; ch < chunks; ch += EPI / 4) {
                 uint32_t v[32];
                 tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN_MAX + ch * 32), v);
                 const int64_t c0 = col0 + ch * 32;
@@ -828,7 +842,7 @@ __global__ void __maxnreg__(128)
                     // Transpose the 32×32 block through shared memory so that each
                     // lane stores 8 consecutive rows of one column as one vector.
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) stg[j * STG_LD + lane] = __uint_as_float(v[j]);
+                    for (int j = 0; j < 32; ++j) stg[stg_idx(j, lane)] = __uint_as_float(v[j]);
                     __syncwarp();
                     const int m = lane & 3;
                     const int64_t r0 = wrow0 + 8 * m;
@@ -838,8 +852,8 @@ __global__ void __maxnreg__(128)
                     for (int rd = 0; rd < 4; ++rd) {
                         const int j = 8 * rd + (lane >> 2);
                         if (j >= ncols || !kr_ok) continue;
-                        const float4 a = *reinterpret_cast<const float4*>(stg + j * STG_LD + 8 * m);
-                        const float4 b = *reinterpret_cast<const float4*>(stg + j * STG_LD + 8 * m + 4);
+                        const float4 a = *reinterpret_cast<const float4*>(stg + stg_idx(j, 8 * m));
+                        const float4 b = *reinterpret_cast<const float4*>(stg + stg_idx(j, 8 * m + 4));
                         const float x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
                         const int64_t qq = c0 + j;
                         if (p.sym != 1 || qq >= pr) store_vec8(p, kr + p.F_pad * pr + p.ldd * qq, x);
@@ -879,7 +893,7 @@ __global__ void __maxnreg__(128)
             if (sym2_mirror && warp_vec) {
                 // the transposed copy, a second pass over the accumulator
                 // (kept apart from the direct stores to bound register use)
-                for (int ch = 0; ch < chunks; ++ch) {
+                for (int ch = cpar; ch < chunks; ch += EPI / 4) {
                     const int64_t c0 = col0 + ch * 32;
                     int64_t ncols = p.M - c0;
                     if (ncols > p.bn - ch * 32) ncols = p.bn - ch * 32;
@@ -986,19 +1000,20 @@ int pad_for(int kind, int64_t n) {
 // Persistent launch of the 2-CTA kernel: one cluster of two per SM pair, capped
 // by how many such clusters the device can hold at once (GPCs with an odd SM
 // count leave one SM out), so that no cluster waits for another to finish.
-template <typename Kern>
-static int launch_pair(Kern kern, int kind, fcb200_context* h, int64_t tiles, const CUtensorMap& a_hi,
-                       const CUtensorMap& a_lo, const CUtensorMap& b_hi, const CUtensorMap& b_lo, const TcParams& p,
-                       cudaStream_t s) {
-    static int max_clusters[2][64] = {};  // per operand kind and device
-    int& slot = max_clusters[kind - 1][h->device & 63];
+template <int KIND, int EPI>
+static int launch_pair(fcb200_context* h, int64_t tiles, const CUtensorMap& a_hi, const CUtensorMap& a_lo,
+                       const CUtensorMap& b_hi, const CUtensorMap& b_lo, const TcParams& p, cudaStream_t s) {
+    auto kern = mode_product_tc2_kernel<KIND, EPI>;
+    constexpr int SMEM2_BYTES = pair_smem_bytes<EPI>();
+    static int max_clusters[64] = {};  // per device, for this kernel
+    int& slot = max_clusters[h->device & 63];
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = 2;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cudaLaunchConfig_t cfg = {};
-    cfg.blockDim = dim3(NUM_THREADS, 1, 1);
+    cfg.blockDim = dim3(pair_threads<EPI>(), 1, 1);
     cfg.dynamicSmemBytes = SMEM2_BYTES;
     cfg.stream = s;
     cfg.attrs = attr;
@@ -1084,8 +1099,14 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
         FCB_TRY(make_map(&pb_hi, B_hi, kind, mp.K, b_rows, mp.ldb, p.bn / 2));
         FCB_TRY(make_map(&pb_lo, B_lo, kind, mp.K, b_rows, mp.ldb, p.bn / 2));
         const int64_t tiles2 = (int64_t)p.m_tiles * p.n_tiles;
-        if (kind == 1) return launch_pair(mode_product_tc2_kernel<1>, 1, h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
-        return launch_pair(mode_product_tc2_kernel<2>, 2, h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
+        // the grouped second product (K of a few hundred) is bound by its
+        // epilogue: twice the epilogue warps
+        if (p.sym == 2) {
+            if (kind == 1) return launch_pair<1, 8>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
+            return launch_pair<2, 8>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
+        }
+        if (kind == 1) return launch_pair<1, 4>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
+        return launch_pair<2, 4>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
     }
     const int64_t tiles = (int64_t)p.m_tiles * p.n_tiles;
     const int grid = (int)(tiles < h->sm_count ? tiles : h->sm_count);
