@@ -200,12 +200,16 @@ int fcb200_mcc3_blocked(fcb200_handle h, const float* psi, const float* phi, int
  *   and mcc3 (src/mcc.jl:29-51)
  * without the host round trip.  psi_out (n³ doubles, unweighted) may be NULL;
  * k3_out holds (mode_hi-mode_lo)³ floats.
- * With a split precision the first two mode products use the block sparsity of
- * the LJ Ψ (non-zeros of the columns of atom K lie in rows and columns of K's
- * neighbourhood): P1 as a sparse contraction, P2 as one GEMM per atom over its
- * neighbours' degrees of freedom; P3 stays dense.  Same K3 within the mcc3
- * tolerance; this form synchronises the stream once (after the neighbour
- * lists).  FCB_MCC3_FORCE_DENSE selects the dense products.
+ * With a split precision the mode products use the block sparsity of the LJ
+ * Ψ (non-zeros of the columns of atom K lie in rows of K's neighbourhood) and
+ * its symmetry: P1 as a sparse contraction that keeps only the neighbourhood
+ * rows, P2 as one GEMM per atom over its neighbours' degrees of freedom
+ * (symmetric in its two mode indices), P3 dense over the atoms with symmetric
+ * tiles — or, where that does not pay (small cells, mode counts not a multiple
+ * of 8), P1 written in the dense layout and symmetric dense P2/P3.  Same K3
+ * within the mcc3 tolerance; this form synchronises the stream once (after the
+ * neighbour lists), and writes psi_out on a second stream beside the last
+ * product.  FCB_MCC3_FORCE_DENSE selects the dense products.
  */
 int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
                        double sigma, double eps, double r_cut, double tol, const double* masses,
@@ -290,8 +294,8 @@ int fcb200_fd_second_order_sw(fcb200_handle h, const double* pos, int64_t n_atom
  * scratch; 0 = 80 % of free memory), the first run executes eagerly and sizes
  * every lane's scratch, and every later run replays the whole batch as ONE
  * CUDA-graph launch on `stream`.  No FP64 Ψ is written.  With a split
- * precision each snapshot runs the block-sparse first mode product and the
- * symmetric P2/P3 of fcb200_snapshot_lj; the sparse tables' capacity is fixed
+ * precision each snapshot runs the sparse mode products of
+ * fcb200_snapshot_lj; the sparse tables' capacity is fixed
  * on the host when the snapshot is added (its largest neighbourhood within
  * r_cut + 0.1 Å, plus 4 atoms) and re-checked by fcb200_batch_set_positions,
  * which re-plans the batch when positions outgrow it.  k3_out must be device
