@@ -59,6 +59,7 @@ struct TcParams {
     int a_mn;                      // A read MN-major through a 3-D map (ModeProduct::a_mn)
     int64_t b_group, b_group_ld;   // ModeProduct::b_group / b_group_ld (pair kernel)
     int64_t Fv;                    // rows r with r % F >= Fv are not stored
+    int tma_out;                   // FP32 output stored by TMA from the staging block (pair kernel)
     void* d_hi;
     void* d_lo;
     int* status;
@@ -622,6 +623,21 @@ __device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* m
         : "memory");
 }
 
+// TMA store of a box from this CTA's shared memory (bulk-group completion).
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int x, int y, int z) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(z), "r"(saddr(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// The staging block may be written again once the TMA engine has read it.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 template <int KIND>
 __device__ __forceinline__ void umma_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     if constexpr (KIND == 1) {
@@ -663,17 +679,20 @@ template <int KIND, int EPI>
 __global__ void __maxnreg__(128)
     mode_product_tc2_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant__ CUtensorMap mA_lo,
                             const __grid_constant__ CUtensorMap mB_hi, const __grid_constant__ CUtensorMap mB_lo,
+                            const __grid_constant__ CUtensorMap mD, const __grid_constant__ CUtensorMap mDt,
                             const TcParams p) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES2 * STAGE2_BYTES);
+    // operand stages, then the epilogue staging blocks (1024-byte aligned, as
+    // the TMA store's 128-byte swizzle wants), then the barriers
+    float* stage_base = reinterpret_cast<float*>(smem + STAGES2 * STAGE2_BYTES);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES2 * STAGE2_BYTES + EPI * 32 * STG_LD * 4);
     uint64_t* empty = full + STAGES2;
     uint64_t* tfull = empty + STAGES2;
     uint64_t* tempty = tfull + 2;
     uint64_t* drain = tempty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-    float* stage_base = reinterpret_cast<float*>(smem + STAGES2 * STAGE2_BYTES + 256);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = cluster_rank();
@@ -838,6 +857,39 @@ __global__ void __maxnreg__(128)
                 int64_t ncols = p.M - c0;  // valid columns of this chunk
                 if (ncols > p.bn - ch * 32) ncols = p.bn - ch * 32;
                 if (ncols > 32) ncols = 32;
+                if (p.tma_out) {
+                    // the staging block may still be read by this warp's last TMA store
+                    if (lane == 0) bulk_wait_read();
+                    __syncwarp();
+                }
+                // a 32-column box may run past the last column of the matrix (the
+                // map clips it) but not into the next mode tile's columns
+                if (p.tma_out && warp_vec && ncols > 0 && (ncols == 32 || c0 + ncols == p.M)) {
+                    // FP32 output by TMA: the warp's 32 rows share one outer index
+                    // pr; a chunk goes whole when every column lies on one side of
+                    // the symmetric diagonal, else by the vector path below
+                    const int64_t pr = wrow0 / p.F, kr0 = wrow0 - pr * p.F;
+                    if (kr0 >= p.Fv) continue;  // padding rows only: nothing is stored
+                    const bool d_all = !p.sym || c0 >= pr, d_none = p.sym && c0 + ncols <= pr;
+                    const bool m_all = p.sym && c0 > pr, m_none = !p.sym || c0 + ncols <= pr + 1;
+                    if ((d_all || d_none) && (m_all || m_none)) {
+                        if (!d_none || !m_none) {
+                            // [column][row], 128-byte lines, 16-byte chunks XOR-swizzled by line
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                stg[j * 32 + ((((lane >> 2) ^ j) & 7) << 2) + (lane & 3)] = __uint_as_float(v[j]);
+                            fence_proxy_async_smem();
+                            __syncwarp();
+                            if (lane == 0) {
+                                if (!d_none) tma_store_3d(&mD, stg, (int)kr0, (int)pr, (int)c0);
+                                if (!m_none) tma_store_3d(&mDt, stg, (int)kr0, (int)c0, (int)pr);
+                                bulk_commit();
+                            }
+                            __syncwarp();
+                        }
+                        continue;
+                    }
+                }
                 if (warp_vec && ncols > 0) {
                     // Transpose the 32×32 block through shared memory so that each
                     // lane stores 8 consecutive rows of one column as one vector.
@@ -911,6 +963,8 @@ __global__ void __maxnreg__(128)
             if (lane == 0) mbar_arrive_cluster(mapa_shared(saddr(&tempty[acc]), 0));
             if (++acc == 2) acc = 0, acc_phase ^= 1;
         }
+        if (p.tma_out && lane == 0) bulk_wait_all();  // this warp's TMA stores complete
+        __syncwarp();
     }
 
     tc_fence_before();
@@ -977,6 +1031,27 @@ int make_map_mn(CUtensorMap* m, const void* base, int kind, int64_t Mx, int64_t 
     return FCB_OK;
 }
 
+// 3-D map of an FP32 output D[(r % F) + F_pad·(r / F) + ldd·c] as (row in
+// block, block, column), boxes of 32 rows × 32 blocks × 1 column or 32 rows ×
+// 1 block × 32 columns, staged in shared memory as 128-byte lines with the
+// 128-byte swizzle.
+int make_map_out(CUtensorMap* m, void* base, int64_t rows, int64_t blocks, int64_t cols, int64_t F_pad, int64_t ldd,
+                 bool box_blocks) {
+    EncodeFn enc = encode_fn();
+    if (!enc) return set_error(FCB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (F_pad * 4) % 16 != 0 || (ldd * 4) % 16 != 0)
+        return set_error(FCB_ERR_ARG, "mode product output is not 16-byte aligned");
+    cuuint64_t dims[3] = {(cuuint64_t)rows, (cuuint64_t)blocks, (cuuint64_t)cols};
+    cuuint64_t strides[2] = {(cuuint64_t)(F_pad * 4), (cuuint64_t)(ldd * 4)};
+    cuuint32_t box[3] = {32, box_blocks ? 32u : 1u, box_blocks ? 1u : 32u};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(FCB_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return FCB_OK;
+}
+
 }  // namespace
 
 // The 2-CTA tile is the default; FCB200_TC_PAIR=0 selects the 1-CTA tile.
@@ -1002,7 +1077,8 @@ int pad_for(int kind, int64_t n) {
 // count leave one SM out), so that no cluster waits for another to finish.
 template <int KIND, int EPI>
 static int launch_pair(fcb200_context* h, int64_t tiles, const CUtensorMap& a_hi, const CUtensorMap& a_lo,
-                       const CUtensorMap& b_hi, const CUtensorMap& b_lo, const TcParams& p, cudaStream_t s) {
+                       const CUtensorMap& b_hi, const CUtensorMap& b_lo, const CUtensorMap& d,
+                       const CUtensorMap& dt, const TcParams& p, cudaStream_t s) {
     auto kern = mode_product_tc2_kernel<KIND, EPI>;
     constexpr int SMEM2_BYTES = pair_smem_bytes<EPI>();
     static int max_clusters[64] = {};  // per device, for this kernel
@@ -1028,7 +1104,7 @@ static int launch_pair(fcb200_context* h, int64_t tiles, const CUtensorMap& a_hi
     if (slot < 0) return set_error(FCB_ERR_UNSUPPORTED, "mode_product_tc: 2-CTA clusters do not fit");
     const int pairs = (int)(tiles < slot ? tiles : slot);
     cfg.gridDim = dim3(2 * pairs, 1, 1);
-    FCB_CUDA(cudaLaunchKernelEx(&cfg, kern, a_hi, a_lo, b_hi, b_lo, p));
+    FCB_CUDA(cudaLaunchKernelEx(&cfg, kern, a_hi, a_lo, b_hi, b_lo, d, dt, p));
     return FCB_OK;
 }
 
@@ -1050,6 +1126,7 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
     p.b_group = mp.b_group;
     p.b_group_ld = mp.b_group_ld;
     p.Fv = mp.Fv > 0 ? mp.Fv : mp.F;
+    p.tma_out = 0;
     if (mp.sym && mp.R != mp.F * mp.M) return set_error(FCB_ERR_ARG, "mode_product_tc: symmetric output needs R = F*M");
     const bool ext = mp.sym_inner || mp.a_mn || mp.b_group || p.Fv != mp.F;
     if (ext) {
@@ -1099,14 +1176,24 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
         FCB_TRY(make_map(&pb_hi, B_hi, kind, mp.K, b_rows, mp.ldb, p.bn / 2));
         FCB_TRY(make_map(&pb_lo, B_lo, kind, mp.K, b_rows, mp.ldb, p.bn / 2));
         const int64_t tiles2 = (int64_t)p.m_tiles * p.n_tiles;
+        // FP32 output with outer symmetry (the third product of the snapshot
+        // paths): the epilogue hands whole 32 × 32 blocks to the TMA engine,
+        // direct and mirrored, when a warp's 32 rows share one outer index
+        CUtensorMap md = ma_hi, mdt = ma_hi;
+        p.tma_out = 0;
+        if (out_kind == 0 && mp.sym && p.vec && mp.F % 32 == 0 && mp.R == mp.F * mp.M) {
+            FCB_TRY(make_map_out(&md, D_hi, p.Fv, mp.M, mp.M, mp.F_pad, mp.ldd, false));
+            FCB_TRY(make_map_out(&mdt, D_hi, p.Fv, mp.M, mp.M, mp.F_pad, mp.ldd, true));
+            p.tma_out = 1;
+        }
         // the grouped second product (K of a few hundred) is bound by its
         // epilogue: twice the epilogue warps
         if (p.sym == 2) {
-            if (kind == 1) return launch_pair<1, 8>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
-            return launch_pair<2, 8>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
+            if (kind == 1) return launch_pair<1, 8>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, md, mdt, p, s);
+            return launch_pair<2, 8>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, md, mdt, p, s);
         }
-        if (kind == 1) return launch_pair<1, 4>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
-        return launch_pair<2, 4>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, p, s);
+        if (kind == 1) return launch_pair<1, 4>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, md, mdt, p, s);
+        return launch_pair<2, 4>(h, tiles2, ma_hi, ma_lo, pb_hi, pb_lo, md, mdt, p, s);
     }
     const int64_t tiles = (int64_t)p.m_tiles * p.n_tiles;
     const int grid = (int)(tiles < h->sm_count ? tiles : h->sm_count);
