@@ -59,7 +59,9 @@ struct TcParams {
     int a_mn;                      // A read MN-major through a 3-D map (ModeProduct::a_mn)
     int64_t b_group, b_group_ld;   // ModeProduct::b_group / b_group_ld (pair kernel)
     int64_t Fv;                    // rows r with r % F >= Fv are not stored
-    int tma_out;                   // FP32 output stored by TMA from the staging block (pair kernel)
+    int tma_out;                   // output stored by TMA from the staging block (pair kernel):
+                                   // 1 = FP32 with outer symmetry (mD direct, mDt mirrored box),
+                                   // 2 = BF16 planes with inner symmetry (mD hi, mDt lo plane)
     void* d_hi;
     void* d_lo;
     int* status;
@@ -310,6 +312,21 @@ __device__ __forceinline__ bool sym_tile_live(const TcParams& p, int mt, int nt)
     return qmax - 1 >= pmin;
 }
 
+// TMA store of a box from this CTA's shared memory (bulk-group completion).
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int x, int y, int z) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(z), "r"(saddr(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// The staging block may be written again once the TMA engine has read it.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // Transposed stores of one 32 × 32 block (inner symmetry): element (row r,
 // column c0 + j) goes to (c0 + j) + F_pad·(r / F) + ldd·(r % F), so the columns
 // of a row are contiguous.  Each lane packs its own row (v[j], j < 32) into the
@@ -323,7 +340,8 @@ __device__ __forceinline__ bool sym_tile_live(const TcParams& p, int mt, int nt)
 // pp0 + row.
 template <int KIND>
 __device__ __forceinline__ void mirror_rows(const TcParams& p, uint8_t* sb, const uint32_t (&v)[32], int lane,
-                                            int64_t pk, int64_t pp0, int64_t c0, int64_t ncols) {
+                                            int64_t pk, int64_t pp0, int64_t c0, int64_t ncols,
+                                            const CUtensorMap* md, const CUtensorMap* mdt) {
     const int64_t base = c0 + p.F_pad * pk + p.ldd * pp0;
     if constexpr (KIND == 1) {
 #pragma unroll
@@ -342,6 +360,21 @@ __device__ __forceinline__ void mirror_rows(const TcParams& p, uint8_t* sb, cons
             const int sw = g ^ ((lane >> 1) & 3);
             *reinterpret_cast<uint4*>(sb + lane * 64 + sw * 16) = make_uint4(h[0], h[1], h[2], h[3]);
             *reinterpret_cast<uint4*>(sb + 2048 + lane * 64 + sw * 16) = make_uint4(l[0], l[1], l[2], l[3]);
+        }
+        if (p.tma_out == 2 && (ncols == 32 || c0 + ncols == p.M)) {
+            // the staging rows are the 64-byte-swizzled box (columns × 1 × rows)
+            // of the planes' map: rows past M and columns past the matrix are
+            // clipped by the map
+            if (pp0 >= p.M) return;  // padding rows only
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) {
+                tma_store_3d(md, sb, (int)c0, (int)pk, (int)pp0);
+                tma_store_3d(mdt, sb + 2048, (int)c0, (int)pk, (int)pp0);
+                bulk_commit();
+            }
+            __syncwarp();
+            return;
         }
         __syncwarp();
 #pragma unroll
@@ -623,21 +656,6 @@ __device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* m
         : "memory");
 }
 
-// TMA store of a box from this CTA's shared memory (bulk-group completion).
-__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int x, int y, int z) {
-    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
-                     reinterpret_cast<uint64_t>(map)),
-                 "r"(x), "r"(y), "r"(z), "r"(saddr(src))
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// The staging block may be written again once the TMA engine has read it.
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 template <int KIND>
 __device__ __forceinline__ void umma_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     if constexpr (KIND == 1) {
@@ -864,7 +882,34 @@ __global__ void __maxnreg__(128)
                 }
                 // a 32-column box may run past the last column of the matrix (the
                 // map clips it) but not into the next mode tile's columns
-                if (p.tma_out && warp_vec && ncols > 0 && (ncols == 32 || c0 + ncols == p.M)) {
+                if constexpr (KIND == 1) {
+                    if (p.tma_out == 2 && warp_vec && ncols > 0 && (ncols == 32 || c0 + ncols == p.M)) {
+                        // BF16 planes by TMA (inner symmetry): [column][row], 64-byte
+                        // lines, 16-byte chunks XOR-swizzled by line pair; every entry
+                        // of a live tile is a direct store
+                        const int64_t pk = wrow0 / p.F, pp0 = wrow0 - pk * p.F;
+                        uint8_t* sb = reinterpret_cast<uint8_t*>(stg);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const float x = __uint_as_float(v[j]);
+                            const __nv_bfloat16 hb = __float2bfloat16_rn(x);
+                            const __nv_bfloat16 lb = __float2bfloat16_rn(x - __bfloat162float(hb));
+                            const int off = j * 64 + ((((lane >> 3) ^ (j >> 1)) & 3) << 4) + (lane & 7) * 2;
+                            *reinterpret_cast<__nv_bfloat16*>(sb + off) = hb;
+                            *reinterpret_cast<__nv_bfloat16*>(sb + 2048 + off) = lb;
+                        }
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) {
+                            tma_store_3d(&mD, sb, (int)pp0, (int)pk, (int)c0);
+                            tma_store_3d(&mDt, sb + 2048, (int)pp0, (int)pk, (int)c0);
+                            bulk_commit();
+                        }
+                        __syncwarp();
+                        continue;
+                    }
+                }
+                if (p.tma_out == 1 && warp_vec && ncols > 0 && (ncols == 32 || c0 + ncols == p.M)) {
                     // FP32 output by TMA: the warp's 32 rows share one outer index
                     // pr; a chunk goes whole when every column lies on one side of
                     // the symmetric diagonal, else by the vector path below
@@ -953,8 +998,12 @@ __global__ void __maxnreg__(128)
                     if (ncols <= 0) break;
                     uint32_t v[32];
                     tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN_MAX + ch * 32), v);
+                    if (p.tma_out) {
+                        if (lane == 0) bulk_wait_read();
+                        __syncwarp();
+                    }
                     mirror_rows<KIND>(p, reinterpret_cast<uint8_t*>(stg), v, lane, wrow0 / p.F, wrow0 % p.F, c0,
-                                      ncols);
+                                      ncols, &mD, &mDt);
                     __syncwarp();
                 }
             }
@@ -1036,17 +1085,20 @@ int make_map_mn(CUtensorMap* m, const void* base, int kind, int64_t Mx, int64_t 
 // 1 block × 32 columns, staged in shared memory as 128-byte lines with the
 // 128-byte swizzle.
 int make_map_out(CUtensorMap* m, void* base, int64_t rows, int64_t blocks, int64_t cols, int64_t F_pad, int64_t ldd,
-                 bool box_blocks) {
+                 bool box_blocks, bool bf16 = false) {
     EncodeFn enc = encode_fn();
     if (!enc) return set_error(FCB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (F_pad * 4) % 16 != 0 || (ldd * 4) % 16 != 0)
+    const int esz = bf16 ? 2 : 4;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (F_pad * esz) % 16 != 0 || (ldd * esz) % 16 != 0)
         return set_error(FCB_ERR_ARG, "mode product output is not 16-byte aligned");
     cuuint64_t dims[3] = {(cuuint64_t)rows, (cuuint64_t)blocks, (cuuint64_t)cols};
-    cuuint64_t strides[2] = {(cuuint64_t)(F_pad * 4), (cuuint64_t)(ldd * 4)};
+    cuuint64_t strides[2] = {(cuuint64_t)(F_pad * esz), (cuuint64_t)(ldd * esz)};
     cuuint32_t box[3] = {32, box_blocks ? 32u : 1u, box_blocks ? 1u : 32u};
     cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+    // 32 elements per line: 128 bytes (FP32) or 64 bytes (BF16), the matching swizzle
+    CUresult r = enc(m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     bf16 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(FCB_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
     return FCB_OK;
@@ -1185,6 +1237,14 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
             FCB_TRY(make_map_out(&md, D_hi, p.Fv, mp.M, mp.M, mp.F_pad, mp.ldd, false));
             FCB_TRY(make_map_out(&mdt, D_hi, p.Fv, mp.M, mp.M, mp.F_pad, mp.ldd, true));
             p.tma_out = 1;
+        }
+        // BF16 planes with inner symmetry (the grouped second product): one map
+        // per plane, (row in block, block, column), serves the direct box and,
+        // with the roles of row and column exchanged, the transposed one
+        if (kind == 1 && out_kind == 1 && mp.sym_inner && p.vec) {
+            FCB_TRY(make_map_out(&md, D_hi, mp.F, mp.R / mp.F, mp.M, mp.F_pad, mp.ldd, false, true));
+            FCB_TRY(make_map_out(&mdt, D_lo, mp.F, mp.R / mp.F, mp.M, mp.F_pad, mp.ldd, false, true));
+            p.tma_out = 2;
         }
         // the grouped second product (K of a few hundred) is bound by its
         // epilogue: twice the epilogue warps
