@@ -38,17 +38,19 @@ def build_oracle(force: bool = False) -> str:
 def build_reference_translation(reference_root: str | None = None, force: bool = False) -> str | None:
     """Translate + compile the reference's generated SW derivative kernels.
 
-    Returns the path of ``oracle/_ref/libswref.so``, or None when the reference
-    sources are not on this machine and no previously built library exists.
+    ``reference_root`` (or the environment variable FCB200_REFERENCE_ROOT) is
+    the ForceConstants.jl checkout; there is no default.  Returns the path of
+    ``oracle/_ref/libswref.so``, or None when no checkout is given or found and
+    no previously built library exists.
     """
     if HERE not in sys.path:
         sys.path.append(HERE)
     from translate_sw_ref import translate_all  # noqa: E402  (sibling module)
 
-    reference_root = reference_root or os.environ.get("FCB200_REFERENCE_ROOT", "/root/reference")
+    reference_root = reference_root or os.environ.get("FCB200_REFERENCE_ROOT")
     lib = os.path.join(REF_OUT, "libswref.so")
-    gen_dir = os.path.join(reference_root, "src", "autodiff", "generated_derivatives")
-    if not os.path.isdir(gen_dir):
+    gen_dir = os.path.join(reference_root, "src", "autodiff", "generated_derivatives") if reference_root else None
+    if gen_dir is None or not os.path.isdir(gen_dir):
         return lib if os.path.exists(lib) else None
     os.makedirs(REF_OUT, exist_ok=True)
     c_path = os.path.join(REF_OUT, "sw_generated.c")
@@ -65,4 +67,5 @@ def build_reference_translation(reference_root: str | None = None, force: bool =
 if __name__ == "__main__":
     sys.path.insert(0, HERE)
     print(build_oracle(force="--force" in sys.argv))
-    print(build_reference_translation(force="--force" in sys.argv))
+    roots = [a for a in sys.argv[1:] if not a.startswith("--")]
+    print(build_reference_translation(roots[0] if roots else None, force="--force" in sys.argv))

@@ -205,6 +205,74 @@ int oracle_third_order_lj(const double* pos, int64_t N, const double box[3], dou
     return 0;
 }
 
+/* The same third_order (ifc.jl:20-35) restricted to the middle-index columns
+ * jj in [j0, j1): out[ii + n*((jj - j0) + w*kk)], w = j1 - j0 (an n × w × n
+ * column-major slab).  The pair loop and its 6-way scatter run as in
+ * oracle_third_order_lj_pairs, dropping only the writes whose middle index
+ * falls outside the slab (every entry is written by exactly one pair
+ * iteration, in the same order as there).  ASR! (asr.jl:19-40) at fixed
+ * (ii, jj) sums along the third index only, so it stays inside the slab;
+ * then apply_tols!.  Equal, entry for entry, to the slab's columns of the
+ * full tensor; it lets large cells (400 atoms: 13.8 GB dense) be checked
+ * slab by slab.  Returns -1 when the r_cut < L assertion would fire. */
+int oracle_third_order_lj_slab(const double* pos, int64_t N, const double box[3], double sigma, double eps,
+                               double r_cut, double tol, int64_t j0, int64_t j1, double* out) {
+    for (int d = 0; d < 3; ++d)
+        if (!(r_cut < box[d])) return -1;
+    const int64_t n = 3 * N, w = j1 - j0;
+    if (j0 < 0 || j1 > n || w <= 0) return -2;
+    memset(out, 0, sizeof(double) * (size_t)(n * w * n));
+    const double rc2 = r_cut * r_cut;
+#define SLAB_SET(x, y, z, v)                                            \
+    do {                                                                \
+        if ((y) >= j0 && (y) < j1) out[(x) + n * (((y) - j0) + w * (int64_t)(z))] = (v); \
+    } while (0)
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t i = 0; i < N; ++i) {
+        for (int64_t j = i + 1; j < N; ++j) {
+            for (int dir = 0; dir < 2; ++dir) {
+                double r[3];
+                for (int x = 0; x < 3; ++x)
+                    r[x] = dir == 0 ? pos[3 * i + x] - pos[3 * j + x] : pos[3 * j + x] - pos[3 * i + x];
+                oracle_nearest_mirror(r, box);
+                double d2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+                if (!(d2 < rc2)) continue;
+                double rn = sqrt(d2), d[4];
+                oracle_lj_derivs(sigma, eps, rn, d);
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        for (int c = 0; c < 3; ++c) {
+                            double val = -oracle_phi3(d, rn, r, a, b, c);
+                            int64_t ii, jj, kk;
+                            if (dir == 0) { ii = 3 * i + a; jj = 3 * i + b; kk = 3 * j + c; }
+                            else          { ii = 3 * i + a; jj = 3 * j + b; kk = 3 * j + c; }
+                            SLAB_SET(ii, jj, kk, val); SLAB_SET(ii, kk, jj, val);
+                            SLAB_SET(jj, kk, ii, val); SLAB_SET(jj, ii, kk, val);
+                            SLAB_SET(kk, ii, jj, val); SLAB_SET(kk, jj, ii, val);
+                        }
+            }
+        }
+    }
+#undef SLAB_SET
+    /* asr.jl:19-40 on the slab's columns (ascending strided sum over kk). */
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t i = 0; i < N; ++i)
+        for (int64_t jj = j0; jj < j1; ++jj)
+            for (int a = 0; a < 3; ++a) {
+                int64_t ii = 3 * i + a;
+                double* col = out + ii + n * (jj - j0);
+                for (int c = 0; c < 3; ++c) {
+                    int64_t kk = 3 * i + c;
+                    col[n * w * kk] = 0.0;
+                    double s = 0.0;
+                    for (int64_t k = c; k < n; k += 3) s += col[n * w * k];
+                    col[n * w * kk] = -s;
+                }
+            }
+    oracle_apply_tols(out, n * w * n, tol);
+    return 0;
+}
+
 int oracle_second_order_lj_full(const double* pos, int64_t N, const double box[3], double sigma,
                                 double eps, double r_cut, double tol, double* ifc2) {
     const int64_t n = 3 * N;

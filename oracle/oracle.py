@@ -41,6 +41,8 @@ def lib():
         L.oracle_third_order_lj.argtypes = [_PD, _I64, _PD, _D, _D, _D, _D, _PD]
         L.oracle_third_order_lj.restype = ctypes.c_int
         L.oracle_third_order_lj_pairs.argtypes = [_PD, _I64, _PD, _D, _D, _D, _PD]
+        L.oracle_third_order_lj_slab.argtypes = [_PD, _I64, _PD, _D, _D, _D, _D, _I64, _I64, _PD]
+        L.oracle_third_order_lj_slab.restype = ctypes.c_int
         L.oracle_second_order_lj_full.argtypes = [_PD, _I64, _PD, _D, _D, _D, _D, _PD]
         L.oracle_second_order_lj_full.restype = ctypes.c_int
         L.oracle_mass_weight3.argtypes = [_PD, _PD, _I64]
@@ -173,6 +175,72 @@ def third_order_lj(pos, box, sigma, eps, r_cut, tol):
     if rc != 0:
         raise ValueError("Cutoff larger than L/2")
     return psi.reshape((n, n, n), order="F")
+
+
+def third_order_lj_slab(pos, box, sigma, eps, r_cut, tol, j0, j1):
+    """The columns jj in [j0, j1) of the middle index of third_order_lj
+    (ifc.jl:20-35): an n × (j1 - j0) × n Fortran array equal, entry for entry,
+    to ``third_order_lj(...)[:, j0:j1, :]`` (lj_oracle.c, oracle_third_order_lj_slab)."""
+    pos, N = _pos(pos)
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    n, w = 3 * N, int(j1) - int(j0)
+    out = np.empty(n * w * n, dtype=np.float64)
+    rc = lib().oracle_third_order_lj_slab(_pd(pos), N, _pd(box), sigma, eps, r_cut, tol, int(j0), int(j1), _pd(out))
+    if rc == -1:
+        raise ValueError("Cutoff larger than L/2")
+    if rc != 0:
+        raise ValueError("slab outside [0, n)")
+    return out.reshape((n, w, n), order="F")
+
+
+def lj_slabs(pos, box, sigma, eps, r_cut, tol, atoms_per_slab=8):
+    """Yields (j0, j1, slab) over the whole middle index, slab by slab."""
+    N = np.asarray(pos).reshape(-1, 3).shape[0]
+    n = 3 * N
+    for a0 in range(0, N, atoms_per_slab):
+        j0, j1 = 3 * a0, min(n, 3 * (a0 + atoms_per_slab))
+        yield j0, j1, third_order_lj_slab(pos, box, sigma, eps, r_cut, tol, j0, j1)
+
+
+def mass_weight_slab(slab, masses, j0, f32=False):
+    """third_order_analytical.jl:185-214 on an n × w × n slab (columns j0..):
+    non-zero entries divided by sqrt((m_i·m_j)·m_k), the oracle's expression;
+    with ``f32`` the weighted values are rounded to FP32 (held in FP64)."""
+    m = np.repeat(np.asarray(masses, dtype=np.float64), 3)
+    n, w = slab.shape[0], slab.shape[1]
+    flat = slab.reshape(-1, order="F")
+    idx = np.flatnonzero(flat)
+    i, rest = idx % n, idx // n
+    j, k = rest % w, rest // w
+    vals = flat[idx] / np.sqrt((m[i] * m[j0 + j]) * m[k])
+    if f32:
+        vals = vals.astype(np.float32).astype(np.float64)
+    out = np.zeros(flat.shape[0])
+    out[idx] = vals
+    return out.reshape(slab.shape, order="F")
+
+
+def mcc3_windows_lj(pos, box, sigma, eps, r_cut, tol, masses, phi, windows, atoms_per_slab=8, f32=True,
+                    on_slab=None):
+    """K3 over mode windows, K3[p, q, s] = Σ_ijk Ψ_mw[i,j,k] φ[i,p] φ[j,q] φ[k,s]
+    for p ∈ P, q ∈ Q, s ∈ S (mcc.jl:29-51 in FP64), accumulated over slabs of
+    the middle index so that the dense Ψ of a large cell is never held whole.
+    Ψ_mw is rounded to FP32 first when ``f32`` (the reference's
+    CuArray{Float32} operand, README.md:73-75).  ``windows`` is a list of
+    (P, Q, S) index arrays; ``on_slab(j0, j1, slab)`` sees every unweighted slab."""
+    phi = np.asarray(phi, dtype=np.float64)
+    outs = [np.zeros((len(P), len(Q), len(S))) for P, Q, S in windows]
+    for j0, j1, slab in lj_slabs(pos, box, sigma, eps, r_cut, tol, atoms_per_slab):
+        if on_slab is not None:
+            on_slab(j0, j1, slab)
+        mw = mass_weight_slab(slab, masses, j0, f32=f32)
+        n, w = mw.shape[0], mw.shape[1]
+        m2 = mw.reshape(n, w * n, order="F")                          # [i, (jl, k)], a view
+        for (P, Q, S), out in zip(windows, outs):
+            t = np.ascontiguousarray(phi[:, P].T) @ m2                # [p, jl + w·k]
+            t = np.matmul(t.reshape(len(P), n, w).transpose(0, 2, 1), phi[:, S])   # [p, jl, s]
+            out += np.einsum("pjs,jq->pqs", t, phi[j0:j1][:, Q], optimize=True)
+    return outs
 
 
 def second_order_lj(pos, box, sigma, eps, r_cut, tol):

@@ -14,7 +14,8 @@
    value) because the dense tensors are mostly zeros.
 
 Run from the repository root on a machine that has the reference checkout:
-``python tests/golden/make_golden.py [reference_root]``.
+``python tests/golden/make_golden.py REFERENCE_ROOT`` (the ForceConstants.jl
+checkout; required).
 """
 from __future__ import annotations
 
@@ -56,4 +57,6 @@ def main(reference_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit(f"usage: python {os.path.basename(__file__)} FORCECONSTANTS_JL_CHECKOUT")
+    main(sys.argv[1])

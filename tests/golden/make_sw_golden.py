@@ -50,4 +50,6 @@ def main(reference_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit(f"usage: python {os.path.basename(__file__)} FORCECONSTANTS_JL_CHECKOUT")
+    main(sys.argv[1])
