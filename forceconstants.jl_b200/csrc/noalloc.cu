@@ -23,8 +23,12 @@
 //    streams, or different host threads) race on the array and must be
 //    serialised by the caller;
 //  * the first call on each device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current.  Make that first call
-//    before any stream capture begins.
+//    (cudaGetSymbolAddress) with that device current, and so does the first
+//    call after that device's context was torn down and created again (for
+//    example by cudaDeviceReset): the address is cached per CUDA context.
+//    Make that first call before any stream capture begins.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "fcb200_internal.cuh"
@@ -43,22 +47,61 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-void* g_addr[kMaxDevices] = {};
+struct ScratchSlot {
+    CUcontext ctx = nullptr;  // context the address belongs to
+    void* addr = nullptr;
+};
+ScratchSlot g_slot[kMaxDevices];
 
-// Device address of the scratch array on the current device (looked up once).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+
+// The driver's cuCtxGetCurrent, through the runtime (no link-time libcuda).
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(p);
+        tried = true;
+    }
+    return fn;
+}
+
+// Device address of the scratch array in the current device's context, looked
+// up on the first call in that context (a context created anew after a reset
+// gets a fresh lookup).  While no context is current on the calling thread yet,
+// or without the driver entry point, it is looked up on every call;
+// cudaGetSymbolAddress itself makes the device's primary context current.
 int scratch_address(void** out) {
     int dev = 0;
     FCB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return set_error(FCB_ERR_ARG, "device index out of range");
+    CUcontext ctx = nullptr;
+    CtxGetCurrentFn get = ctx_get_current();
+    const bool known = get != nullptr && get(&ctx) == CUDA_SUCCESS && ctx != nullptr;
     std::lock_guard<std::mutex> lock(g_mu);
-    if (g_addr[dev] == nullptr) {
+    ScratchSlot& slot = g_slot[dev];
+    if (!known || slot.addr == nullptr || slot.ctx != ctx) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(no-alloc scratch)");
-        g_addr[dev] = p;
+        slot.addr = p;
+        slot.ctx = known ? ctx : nullptr;
     }
-    *out = g_addr[dev];
+    *out = slot.addr;
     return FCB_OK;
+}
+
+// The three box lengths, passed by value, written into the scratch array.
+__global__ void put_box_kernel(double* d_box, double bx, double by, double bz) {
+    if (threadIdx.x == 0) {
+        d_box[0] = bx;
+        d_box[1] = by;
+        d_box[2] = bz;
+    }
 }
 
 int require_device(const void* p, const char* name) {
@@ -108,7 +151,8 @@ extern "C" int fcb200_third_order_lj_noalloc(const double* pos, int64_t n_atoms,
     double* T = reinterpret_cast<double*>(b + kTOff);
     double* S = reinterpret_cast<double*>(b + kSOff);
     uint8_t* flag = reinterpret_cast<uint8_t*>(b + kFlagOff);
-    FCB_CUDA(cudaMemcpyAsync(d_box, box, 3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    put_box_kernel<<<1, 32, 0, s>>>(d_box, box[0], box[1], box[2]);
+    FCB_CUDA(cudaGetLastError());
     FCB_TRY(lj_pair_tables_raw(T, flag, S, pos, n_atoms, d_box, sigma, eps, r_cut, s));
     AssemblyOut out;
     out.psi64 = psi_out;

@@ -341,7 +341,9 @@ int fcb200_phase_times(fcb200_handle h, double* ms, int max_phases);
  *    and it keeps the last call's contents (nothing in it needs to start at
  *    zero); calls that overlap on the GPU race on it and must be serialised;
  *  - the first call on a device looks up the array's address with that device
- *    current; make that first call before any stream capture begins.
+ *    current (again after the device's context was reset: the address is
+ *    cached per CUDA context); make that first call before any stream capture
+ *    begins.
  * Asynchronous on `stream`.
  */
 #define FCB_NOALLOC_MAX_ATOMS 256

@@ -10,7 +10,8 @@ two different systems in a row: the second call must not be affected by what
 the first one left in the shared array.
 
 The file name sorts last so that a run stopping at the first failure has run
-every other test before this one.
+every other test before this one.  A further test queues two calls on one
+non-default stream with no host synchronisation between them.
 """
 import ctypes
 
@@ -94,3 +95,36 @@ def test_noalloc_rejects_oversize_and_host_buffers(fcb, cuda_device):
                                          AR["r_cut"], 1e-12, None, host_out.ctypes.data, None, 0, None)
     assert st == _lib.FCB_ERR_ARG
     assert "device memory" in _lib.last_error()[1]
+
+
+def test_noalloc_back_to_back_on_one_stream(fcb, cuda_device):
+    """Two calls of different sizes queued on one non-default stream with no
+    host synchronisation between them — the way the shared scratch is meant to
+    be used, since calls on one stream run one after the other — and a single
+    synchronisation at the end: both results equal the regular entry point."""
+    import torch
+    from fcb200 import _lib
+    from fcb200.arrays import julia_empty
+    L = _lib.lib()
+    s1, s2 = fcc_system((4, 4, 4), 0.04, 303), fcc_system((3, 3, 3), 0.06, 404)
+    m1, m2 = np.full(s1.n_atoms, 39.95), np.linspace(30.0, 50.0, s2.n_atoms)
+    stream = torch.cuda.Stream()
+    outs = []
+    with torch.cuda.stream(stream):
+        for s, m in ((s1, m1), (s2, m2)):
+            n = 3 * s.n_atoms
+            pos = torch.from_numpy(s.positions).cuda()
+            dm = torch.from_numpy(m).cuda()
+            psi = julia_empty((n, n, n), np.float64, "cuda")
+            psi32 = julia_empty((n, n, n), np.float32, "cuda")
+            box = np.ascontiguousarray(s.box_sizes)
+            _lib.check(L.fcb200_third_order_lj_noalloc(
+                int(pos.data_ptr()), s.n_atoms, box.ctypes.data, AR["sigma"], AR["eps"], AR["r_cut"], 1e-12,
+                int(dm.data_ptr()), int(psi.data_ptr()), int(psi32.data_ptr()), 0,
+                ctypes.c_void_p(stream.cuda_stream)))
+            outs.append((pos, dm, psi, psi32))
+    stream.synchronize()
+    for (s, m), (_, _, psi, psi32) in zip(((s1, m1), (s2, m2)), outs):
+        r64, r32 = _regular(fcb, s, m, 0, True)
+        assert np.array_equal(psi.cpu().numpy(), r64)
+        assert np.array_equal(psi32.cpu().numpy(), r32)
