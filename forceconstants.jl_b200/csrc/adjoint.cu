@@ -5,7 +5,8 @@
 // Ψ_mw[i,j,k] = Ψ[i,j,k]/sqrt(m_i m_j m_k) and K3 = Ψ_mw ×₁ φ ×₂ φ ×₃ φ,
 //     L = Σ_ijk G[i,j,k] Ψ_mw[i,j,k],   G = W ×₁ φᵀ ×₂ φᵀ ×₃ φᵀ,
 // i.e. the three transposed mode products of mcc3 (src/mcc.jl:29-51) applied
-// to W.  G runs on the same mode-product kernels (tensor cores or FP32).
+// to W.  G runs on the same mode-product kernels (tensor cores or FP32), or in
+// FP64 on the DFMA mode product (FCB_ADJOINT_FP64).
 //
 // For the analytical LJ calculator every non-zero Ψ block belongs to one
 // ordered pair (A,B) inside the cutoff: the blocks with two A's and one B hold
@@ -83,10 +84,11 @@ __device__ __forceinline__ double phi4_of(const LJRad& f, const double nh[3], do
            (dl(a, b) * dl(c, d) + dl(a, c) * dl(b, d) + dl(a, d) * dl(b, c)) * E2;
 }
 
-// one thread per ordered pair (A,B): v_AB, (∂ϕ₃/∂σ)·C, ϕ₃·C
+// one thread per ordered pair (A,B): v_AB, (∂ϕ₃/∂σ)·C, ϕ₃·C; G in FP32 or FP64
+template <class GT>
 __global__ void lj_adjoint_pair_kernel(const double* __restrict__ pos, const double* __restrict__ box, int64_t N,
                                        double sigma, double eps, double rc2, const double* __restrict__ masses,
-                                       const float* __restrict__ G, double* __restrict__ V, double* __restrict__ Sg,
+                                       const GT* __restrict__ G, double* __restrict__ V, double* __restrict__ Sg,
                                        double* __restrict__ Lp) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= N * N) return;
@@ -171,13 +173,34 @@ __global__ void lj_adjoint_sum_kernel(int64_t NN, const double* __restrict__ Sg,
 
 }  // namespace
 
-// G = W ×₁ φᵀ ×₂ φᵀ ×₃ φᵀ with W (M×M×M) and φ (n×n, modes [0,M)): output n³.
+// G = W ×₁ φᵀ ×₂ φᵀ ×₃ φᵀ with W (M×M×M) and φ (n×n, modes [0,M)): output n³
+// (doubles for FCB_ADJOINT_FP64, floats otherwise).
 int adjoint_g(fcb200_context* h, int precision, const float* d_W, int64_t M, const float* d_phi, int64_t n,
-              float* d_G, cudaStream_t s) {
+              void* d_Gv, cudaStream_t s) {
     FCB_TRY(h->adj_phiT.ensure(sizeof(float) * (size_t)(n * M)));
     float* phiT = h->adj_phiT.as<float>();
     transpose_kernel<<<(unsigned)((n * M + 255) / 256), 256, 0, s>>>(d_phi, n, M, phiT);
     FCB_CUDA(cudaGetLastError());
+    if (precision == FCB_ADJOINT_FP64) {
+        // W and φᵀ widened exactly to FP64; intermediates and G in FP64.
+        FCB_TRY(h->adj_w64.ensure(sizeof(double) * (size_t)(M * M * M)));
+        FCB_TRY(h->adj_phiT64.ensure(sizeof(double) * (size_t)(n * M)));
+        FCB_TRY(h->u1_f32.ensure(sizeof(double) * (size_t)(M * M * n)));
+        FCB_TRY(h->u2_f32.ensure(sizeof(double) * (size_t)(M * n * n)));
+        double* w64 = h->adj_w64.as<double>();
+        double* pt64 = h->adj_phiT64.as<double>();
+        double* u1 = h->u1_f32.as<double>();
+        double* u2 = h->u2_f32.as<double>();
+        FCB_TRY(widen_f32_to_f64(d_W, w64, M * M * M, s));
+        FCB_TRY(widen_f32_to_f64(phiT, pt64, n * M, s));
+        ModeProduct p1{M * M, M, n, M, M, M, M, M * M};
+        FCB_TRY(mode_product_f64(w64, pt64, u1, p1, s));
+        ModeProduct p2{M * n, M, n, M, M, M, M, M * n};
+        FCB_TRY(mode_product_f64(u1, pt64, u2, p2, s));
+        ModeProduct p3{n * n, M, n, M, M, n * n, n * n, n * n};
+        return mode_product_f64(u2, pt64, static_cast<double*>(d_Gv), p3, s);
+    }
+    float* d_G = static_cast<float*>(d_Gv);
     if (precision == FCB_MCC3_FP32) {
         FCB_TRY(h->u1_f32.ensure(sizeof(float) * (size_t)(M * M * n)));
         FCB_TRY(h->u2_f32.ensure(sizeof(float) * (size_t)(M * n * n)));
@@ -214,15 +237,20 @@ int adjoint_g(fcb200_context* h, int precision, const float* d_W, int64_t M, con
 }
 
 int lj_adjoint_pairs(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
-                     double eps, double r_cut, const double* d_masses, const float* d_G, double* d_dpos,
+                     double eps, double r_cut, const double* d_masses, const void* d_G, bool g64, double* d_dpos,
                      double* d_scal, cudaStream_t s) {
     const int64_t NN = N * N;
     FCB_TRY(h->adj_pairs.ensure(sizeof(double) * (size_t)(5 * NN)));
     double* V = h->adj_pairs.as<double>();
     double* Sg = V + 3 * NN;
     double* Lp = Sg + NN;
-    lj_adjoint_pair_kernel<<<(unsigned)((NN + 127) / 128), 128, 0, s>>>(d_pos, d_box, N, sigma, eps, r_cut * r_cut,
-                                                                         d_masses, d_G, V, Sg, Lp);
+    const unsigned blocks = (unsigned)((NN + 127) / 128);
+    if (g64)
+        lj_adjoint_pair_kernel<double><<<blocks, 128, 0, s>>>(d_pos, d_box, N, sigma, eps, r_cut * r_cut, d_masses,
+                                                              static_cast<const double*>(d_G), V, Sg, Lp);
+    else
+        lj_adjoint_pair_kernel<float><<<blocks, 128, 0, s>>>(d_pos, d_box, N, sigma, eps, r_cut * r_cut, d_masses,
+                                                             static_cast<const float*>(d_G), V, Sg, Lp);
     lj_adjoint_atom_kernel<<<(unsigned)((3 * N + 127) / 128), 128, 0, s>>>(N, V, d_dpos);
     lj_adjoint_sum_kernel<<<1, 256, 0, s>>>(NN, Sg, Lp, eps, d_scal);
     FCB_CUDA(cudaGetLastError());

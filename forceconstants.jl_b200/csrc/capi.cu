@@ -278,7 +278,8 @@ int fcb200_trim(fcb200_handle h) {
                    &h->k3_stage[1], &h->ifc2, &h->sw_ints, &h->sw_nbr_r, &h->sw_pair_off, &h->sw_blk3,
                    &h->sw_blk2, &h->sw_atoms, &h->sw_place, &h->sw_col_off, &h->sw_col_items, &h->sw_cursor,
                    &h->sw_asr_off, &h->sw_asr_items, &h->sw_asr, &h->adj_phiT, &h->adj_w_hi, &h->adj_w_lo,
-                   &h->adj_pairs, &h->adj_G, &h->adj_scal, &h->adj_w32, &h->adj_dpos, &h->eig_a, &h->eig_w,
+                   &h->adj_pairs, &h->adj_G, &h->adj_scal, &h->adj_w32, &h->adj_dpos, &h->adj_w64,
+                   &h->adj_phiT64, &h->eig_a, &h->eig_w,
                    &h->eig_work, &h->sp_ints, &h->sp_coef, &h->phik_hi, &h->phik_lo, &h->fd_elems, &h->fd_out};
     for (Buf* b : bufs) b->release();
     return FCB_OK;
@@ -900,7 +901,8 @@ int fcb200_mcc3_adjoint_lj(fcb200_handle h, const double* pos, int64_t N, const 
     if (!phi || !W || !dpos) return set_error(FCB_ERR_ARG, "phi, W and dpos must not be NULL");
     const int64_t n = 3 * N;
     if (n_modes < 1 || n_modes > n) return set_error(FCB_ERR_ARG, "n_modes must be in [1, 3*n_atoms]");
-    FCB_TRY(check_precision(precision));
+    const bool g64 = precision == FCB_ADJOINT_FP64;
+    if (!g64) FCB_TRY(check_precision(precision));
     double bh[3];
     FCB_TRY(box_to_host(box, bh));
     FCB_TRY(check_cutoff(bh));
@@ -916,10 +918,10 @@ int fcb200_mcc3_adjoint_lj(fcb200_handle h, const double* pos, int64_t N, const 
     FCB_TRY(device_view(h->phi_f32, phi, (size_t)(n * n), true, s, &d_phi));
     FCB_TRY(device_view(h->adj_w32, W, (size_t)(n_modes * n_modes * n_modes), true, s, &d_W));
     FCB_TRY(device_view(h->adj_dpos, (const double*)dpos, (size_t)(3 * N), false, s, &d_dpos));
-    FCB_TRY(h->adj_G.ensure(sizeof(float) * (size_t)(n * n * n)));
+    FCB_TRY(h->adj_G.ensure((g64 ? sizeof(double) : sizeof(float)) * (size_t)(n * n * n)));
     FCB_TRY(h->adj_scal.ensure(sizeof(double) * 4));
-    FCB_TRY(adjoint_g(h, precision, d_W, n_modes, d_phi, n, h->adj_G.as<float>(), s));
-    FCB_TRY(lj_adjoint_pairs(h, d_pos, N, d_box, sigma, eps, r_cut, d_m, h->adj_G.as<float>(), d_dpos,
+    FCB_TRY(adjoint_g(h, precision, d_W, n_modes, d_phi, n, h->adj_G.p, s));
+    FCB_TRY(lj_adjoint_pairs(h, d_pos, N, d_box, sigma, eps, r_cut, d_m, h->adj_G.p, g64, d_dpos,
                              h->adj_scal.as<double>(), s));
     double sc[3];
     FCB_CUDA(cudaMemcpyAsync(sc, h->adj_scal.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -82,6 +82,7 @@ struct fcb200_context {
     fcb::Buf sw_col_off, sw_col_items, sw_cursor, sw_asr_off, sw_asr_items, sw_asr;
     // adjoint scratch
     fcb::Buf adj_phiT, adj_w_hi, adj_w_lo, adj_pairs, adj_G, adj_scal, adj_w32, adj_dpos;
+    fcb::Buf adj_w64, adj_phiT64;   // FP64 forms of W and φᵀ (FCB_ADJOINT_FP64)
     // block-sparse P1 of the LJ snapshot: neighbour lists and coefficient tables
     fcb::Buf sp_ints, sp_coef;
     fcb::Buf phik_hi, phik_lo;      // compact sparse form: per-atom φ rows (split)
@@ -172,10 +173,11 @@ int snapshot_lj_device(fcb200_context* h, const double* d_pos, int64_t N, const 
                        int64_t mode_hi, int precision, float* d_k3, cudaStream_t s);
 
 // Adjoint (adjoint.cu)
+// G is FP64 (n³ doubles) for FCB_ADJOINT_FP64, FP32 otherwise.
 int adjoint_g(fcb200_context* h, int precision, const float* d_W, int64_t M, const float* d_phi, int64_t n,
-              float* d_G, cudaStream_t s);
+              void* d_G, cudaStream_t s);
 int lj_adjoint_pairs(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
-                     double eps, double r_cut, const double* d_masses, const float* d_G, double* d_dpos,
+                     double eps, double r_cut, const double* d_masses, const void* d_G, bool g64, double* d_dpos,
                      double* d_scal, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
@@ -212,6 +214,9 @@ struct ModeProduct {
 
 int mode_product_f32(const float* A, const float* B, float* D, const ModeProduct& mp,
                      cudaStream_t s);
+// FP64 (DFMA) mode product and an FP32 → FP64 widening copy (mode_product_f64.cu).
+int mode_product_f64(const double* A, const double* B, double* D, const ModeProduct& mp, cudaStream_t s);
+int widen_f32_to_f64(const float* src, double* dst, int64_t count, cudaStream_t s);
 // Finite-difference IFCs (finite_diff.cu).  kind 0 = LJ, 1 = SW.
 int fd_third_order_launch(const double* d_pos, const double* d_box, int64_t N, int kind, double sigma, double eps,
                           double r_cut, const int64_t* d_elems, int64_t m, double h, double* d_out, cudaStream_t s);

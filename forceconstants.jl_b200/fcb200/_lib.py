@@ -24,8 +24,11 @@ FCB_ERR_BLOCK = 7
 FCB_MCC3_FP32 = 0
 FCB_MCC3_BF16X3 = 1
 FCB_MCC3_TF32X3 = 2
+FCB_ADJOINT_FP64 = 3
 FCB_MCC3_FORCE_DENSE = 0x100
 PRECISIONS = {"fp32": FCB_MCC3_FP32, "bf16x3": FCB_MCC3_BF16X3, "tf32x3": FCB_MCC3_TF32X3}
+# The adjoint also forms G in FP64 (FCB_ADJOINT_FP64).
+ADJOINT_PRECISIONS = dict(PRECISIONS, fp64=FCB_ADJOINT_FP64)
 
 FCB_PSI_MASS_WEIGHTED = 1
 

@@ -48,6 +48,8 @@ extern "C" {
 #define FCB_MCC3_FP32       0  /* plain FP32 SIMT mode products (FFMA)                     */
 #define FCB_MCC3_BF16X3     1  /* split-BF16 on tcgen05: hi·hi + hi·lo + lo·hi, FP32 acc   */
 #define FCB_MCC3_TF32X3     2  /* split-TF32 on tcgen05: hi·hi + hi·lo + lo·hi, FP32 acc   */
+/* fcb200_mcc3_adjoint_lj only: G = W ×₁φᵀ ×₂φᵀ ×₃φᵀ formed in FP64 (DFMA)    */
+#define FCB_ADJOINT_FP64    3
 /* OR into the precision of fcb200_snapshot_lj: run the dense first and second
  * mode products even where the block-sparse form applies.                     */
 #define FCB_MCC3_FORCE_DENSE 0x100
@@ -237,7 +239,9 @@ int fcb200_snapshot_sw(fcb200_handle h, const double* pos, int64_t n_atoms, cons
  * their fourth derivatives ϕ₄ (fourth_order_analytical.jl:184-198) and
  * σ-derivatives with G; Ψ and the fourth-order tensor are never stored.  The
  * tolerance cutoff of Ψ is not differentiated.  W is n_modes³ floats,
- * column-major.  Synchronises the stream.
+ * column-major.  precision: FCB_MCC3_FP32 / _BF16X3 / _TF32X3, or
+ * FCB_ADJOINT_FP64 (G in double precision: the gradient then carries FP64
+ * rounding only).  Synchronises the stream.
  */
 int fcb200_mcc3_adjoint_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
                            double sigma, double eps, double r_cut, const double* masses,

@@ -3,8 +3,10 @@
 Checks ∂L/∂positions, ∂L/∂σ, ∂L/∂ε for L = Σ W·K3 (φ frozen) against
 (1) the FP64 pair-form adjoint of the oracle and (2) central finite
 differences of the FP64 reference path (h = 1e-5 Å for positions, 1e-6
-relative for σ and ε).  Tolerance: 1e-6 relative (normwise over the checked
-components) for the FP32 and TF32×3 forms of G; 1e-4 for BF16×3.
+relative for σ and ε), on a 32-atom cell and at the differentiation
+configuration (256 atoms, W over the first 256 modes, all 768 position
+components).  Tolerance: 1e-6 relative (normwise over the checked components)
+for the FP64, FP32 and TF32×3 forms of G; 1e-4 for BF16×3.
 """
 import numpy as np
 import pytest
@@ -71,49 +73,73 @@ def test_adjoint_vs_central_differences(fcb, oracle, cuda_device, small):
     assert abs(fde - out["deps"]) <= 1e-6 * abs(fde)
 
 
-def test_adjoint_at_scale_vs_central_differences(fcb, cuda_device):
-    """The 256-atom cell, modes 0..63: the adjoint against central differences
-    of L evaluated with the GPU's bit-exact FP64 Ψ and an FP64 contraction on
-    the device (h = 2e-3 Å on atoms clear of the LJ truncation; 1e-6 relative
-    for σ).  Tolerance 1e-5 of the largest component."""
+def _config5_reference(fcb, cuda_device):
+    """The differentiation configuration: the 256-atom displaced cell of the
+    precision configuration (std 0.05 Å, seed 1234, tol 1e-12), φ frozen (FP32
+    modes of its dynamical matrix, from the device), W ~ N(0,1) over the first
+    256 modes on every axis (seeded).  L is linear in the mass-weighted Ψ,
+    L(x) = Σ G[i,j,k] Ψ(x)[i,j,k] / sqrt(m_i m_j m_k) with G = W ×₁φᵀ ×₂φᵀ ×₃φᵀ,
+    so the reference L is evaluated with G formed once in FP64 (torch, on the
+    device) and the GPU's FP64 Ψ, which is bit-exact to the oracle."""
     import torch
-    from fcb200.adjoint import mcc3_adjoint_lj
-    from conftest import atoms_clear_of_cutoff
     s = fcc_system((4, 4, 4), 0.05, 1234)
     pot = fcb.LJ(AR["sigma"], AR["eps"], AR["r_cut"])
-    calc = fcb.AnalyticalCalculator(0.0, AR["r_cut"])
-    n, M = 3 * s.n_atoms, 64
+    calc = fcb.AnalyticalCalculator(1e-12, AR["r_cut"])
+    M = 256
     dyn = fcb.dynamical_matrix(s, pot, calc, device="cuda")
     _, _, phi = fcb.get_modes(dyn, 3, phi32=True)
-    phi64 = phi[:, :M].double()
-    W = torch.from_numpy(np.random.default_rng(9).normal(size=(M, M, M))).to(cuda_device)
-    inv_sqrt_m = torch.from_numpy(np.repeat(s.masses, 3) ** -0.5).to(cuda_device)
+    W32 = np.asfortranarray(np.random.default_rng(2025).normal(size=(M, M, M)).astype(np.float32))
+    ph = phi[:, :M].double()
+    W = torch.from_numpy(np.ascontiguousarray(W32.astype(np.float64))).to(cuda_device)   # [p,q,s] logical
+    g = torch.tensordot(ph, W, dims=([1], [0]))          # [i, q, s]
+    g = torch.tensordot(g, ph, dims=([1], [1]))          # [i, s, j]
+    g = torch.tensordot(g, ph, dims=([1], [1]))          # [i, j, k]
+    w = torch.from_numpy(np.repeat(s.masses, 3) ** -0.5).to(cuda_device)
+    gw = g * w[:, None, None] * w[None, :, None] * w[None, None, :]
+    del g
+    flat = gw.permute(2, 1, 0).contiguous().reshape(-1)  # column-major memory order, as Ψ
+    del gw
 
-    def L(sys_, sigma=pot.sigma):
-        p = fcb.LJ(sigma, pot.eps, pot.r_cut)
-        psi = fcb.third_order(sys_, p, calc, device="cuda").values          # n×n×n column-major FP64
-        t = psi.permute(2, 1, 0)                                            # [k][j][i] row-major view
-        t = t * inv_sqrt_m[None, None, :] * inv_sqrt_m[None, :, None] * inv_sqrt_m[:, None, None]
-        k3 = torch.einsum("kji,ip,jq,ks->pqs", t, phi64, phi64, phi64)
-        return float((k3 * W.permute(0, 1, 2)).sum())   # W[p,q,s] against K3[p,q,s]
+    def L(pos, sigma=pot.sigma, eps=pot.eps):
+        sys_ = fcb.SuperCellSystem(pos, s.masses, s.box_sizes)
+        psi = fcb.third_order(sys_, fcb.LJ(sigma, eps, pot.r_cut), calc, device="cuda").values
+        return float(torch.dot(psi.permute(2, 1, 0).reshape(-1), flat))
 
-    W32 = np.asfortranarray(W.cpu().numpy().astype(np.float32))
-    phi32 = np.asfortranarray(phi.cpu().numpy())
-    out = mcc3_adjoint_lj(s, pot, calc, phi32, W32, precision="tf32x3")
-    clear = atoms_clear_of_cutoff(s, AR["r_cut"])
-    h = 2e-3
-    fd, ad = [], []
-    for a, d in [(int(clear[0]), 0), (int(clear[7]), 1), (int(clear[31]), 2), (int(clear[60]), 0)]:
-        pp = s.positions.copy()
-        pp.reshape(-1, 3)[a, d] += h
-        lp = L(fcb.SuperCellSystem(pp, s.masses, s.box_sizes))
-        pp.reshape(-1, 3)[a, d] -= 2 * h
-        lm = L(fcb.SuperCellSystem(pp, s.masses, s.box_sizes))
-        fd.append((lp - lm) / (2 * h))
-        ad.append(out["dpos"][a, d])
-    scale = np.max(np.abs(out["dpos"]))
-    assert np.max(np.abs(np.array(fd) - np.array(ad))) <= 1e-5 * scale
+    return s, pot, calc, phi.cpu().numpy(), W32, L
+
+
+def test_adjoint_config5_vs_central_differences(fcb, cuda_device):
+    """All 768 position components, σ and ε of the differentiation
+    configuration against central differences (h = 1e-5 Å; 1e-6 relative for
+    σ and ε) of the FP64 L, with G formed in FP64 by the adjoint.  Tolerance
+    1e-6 relative: max over the components of |AD − FD| / max |FD|, and
+    |AD − FD| / |FD| for σ and ε."""
+    from fcb200.adjoint import mcc3_adjoint_lj
+    s, pot, calc, phi32, W32, L = _config5_reference(fcb, cuda_device)
+    out = mcc3_adjoint_lj(s, pot, calc, phi32, W32, precision="fp64")
+    L0 = L(s.positions)
+    assert abs(out["L"] - L0) <= 1e-10 * abs(L0)
+    h = 1e-5
+    fd = np.zeros_like(s.positions)
+    for a in range(s.n_atoms):
+        for d in range(3):
+            p = s.positions.copy()
+            p[a, d] += h
+            lp = L(p)
+            p[a, d] -= 2 * h
+            fd[a, d] = (lp - L(p)) / (2 * h)
+    err = np.max(np.abs(out["dpos"] - fd)) / np.max(np.abs(fd))
+    assert err <= 1e-6, err
     hs = 1e-6 * pot.sigma
-    fds = (L(s, pot.sigma + hs) - L(s, pot.sigma - hs)) / (2 * hs)
-    assert abs(fds - out["dsigma"]) <= 1e-5 * abs(fds)
-    assert abs(out["deps"] - out["L"] / pot.eps) <= 1e-9 * abs(out["deps"])
+    fds = (L(s.positions, pot.sigma + hs) - L(s.positions, pot.sigma - hs)) / (2 * hs)
+    assert abs(out["dsigma"] - fds) <= 1e-6 * abs(fds), (out["dsigma"], fds)
+    he = 1e-6 * pot.eps
+    fde = (L(s.positions, pot.sigma, pot.eps + he) - L(s.positions, pot.sigma, pot.eps - he)) / (2 * he)
+    assert abs(out["deps"] - fde) <= 1e-6 * abs(fde), (out["deps"], fde)
+    # the single-precision forms of G against the FP64 form (the FD check above
+    # pins the FP64 form to 1e-6)
+    for precision, tol in (("tf32x3", 1e-6), ("fp32", 1e-6)):
+        o = mcc3_adjoint_lj(s, pot, calc, phi32, W32, precision=precision)
+        e = np.max(np.abs(o["dpos"] - out["dpos"])) / np.max(np.abs(out["dpos"]))
+        assert e <= tol, (precision, e)
+        assert abs(o["dsigma"] - out["dsigma"]) <= tol * abs(out["dsigma"]), precision
