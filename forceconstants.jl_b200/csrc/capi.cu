@@ -307,6 +307,12 @@ int fcb200_synchronize(fcb200_handle h, void* stream) {
     return check_status(h, static_cast<cudaStream_t>(stream));
 }
 
+int fcb200_set_wait_limit(fcb200_handle h, int64_t limit_ns) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    h->wait_limit_ns = limit_ns > 0 ? (uint64_t)limit_ns : 2000000000ull;
+    return FCB_OK;
+}
+
 int fcb200_set_profiling(fcb200_handle h, int enable) {
     if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
     cudaSetDevice(h->device);

@@ -47,7 +47,10 @@ constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
 constexpr int TMEM_COLS = 2 * BN_MAX;
 constexpr int NUM_THREADS = 192;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr uint64_t TIMEOUT_NS = 2000000000ull;  // 2 s per wait
+// Drains on the abort path (copies and MMAs already issued) always get 2 s,
+// whatever the limit of the ordinary waits (TcParams::wait_ns, 2 s by
+// default), so that nothing is in flight when the CTA frees TMEM and exits.
+constexpr uint64_t DRAIN_NS = 2000000000ull;
 
 struct TcParams {
     int64_t R, K, M;
@@ -65,6 +68,7 @@ struct TcParams {
     void* d_hi;
     void* d_lo;
     int* status;
+    uint64_t wait_ns;              // limit of every ordinary mbarrier wait
 };
 
 __device__ __forceinline__ uint32_t saddr(const void* p) {
@@ -94,15 +98,17 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
 }
 
 // Bounded wait.  Returns false (after flagging the CTA and the device status
-// word) when the phase does not complete within TIMEOUT_NS, or when another
-// role of this CTA has already given up (unless `ignore_abort`).
+// word) when the phase does not complete within `limit_ns`, or when another
+// role of this CTA has already given up (unless `ignore_abort`, the drains,
+// which always wait up to DRAIN_NS).
 __device__ __noinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, volatile int* abort_flag, int* status,
-                                            int code, bool ignore_abort) {
+                                            int code, bool ignore_abort, uint64_t limit_ns) {
     const uint64_t t0 = gtimer();
+    const uint64_t lim = ignore_abort ? DRAIN_NS : limit_ns;
     while (true) {
         if (mbar_try(b, parity)) return true;
         if (!ignore_abort && *abort_flag) return false;
-        if (gtimer() - t0 > TIMEOUT_NS) {
+        if (gtimer() - t0 > lim) {
             *abort_flag = 1;
             atomicCAS(status, 0, code);
             return false;
@@ -111,9 +117,9 @@ __device__ __noinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, volati
 }
 
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag, int* status,
-                                          int code, bool ignore_abort = false) {
+                                          int code, uint64_t limit_ns, bool ignore_abort = false) {
     if (mbar_try(b, parity)) return true;
-    return mbar_wait_slow(b, parity, abort_flag, status, code, ignore_abort);
+    return mbar_wait_slow(b, parity, abort_flag, status, code, ignore_abort, limit_ns);
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
@@ -469,7 +475,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
                 const int nt = t % p.n_tiles, mt = t / p.n_tiles;
                 for (int kc = 0; kc < p.k_chunks; ++kc) {
-                    if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_PRODUCER)) {
+                    if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_PRODUCER, p.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -490,7 +496,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 for (int s = 0; s < STAGES; ++s)
                     if (filled & (1u << s))
                         mbar_wait(&full[s], (filled_phase >> s) & 1u, abort_flag, p.status, DEV_TIMEOUT_PRODUCER,
-                                  true);
+                                  p.wait_ns, true);
             }
         }
         __syncwarp();
@@ -502,14 +508,14 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             uint32_t phase = 0, acc_phase = 0;
             bool ok = true, issued = false;
             for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-                if (!mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_MMA)) {
+                if (!mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_MMA, p.wait_ns)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
                 const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN_MAX);
                 for (int kc = 0; kc < p.k_chunks; ++kc) {
-                    if (!mbar_wait(&full[stage], phase, abort_flag, p.status, DEV_TIMEOUT_MMA)) {
+                    if (!mbar_wait(&full[stage], phase, abort_flag, p.status, DEV_TIMEOUT_MMA, p.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -536,7 +542,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             if ((!ok || *abort_flag) && issued) {
                 // Wait for every MMA this thread issued before TMEM is freed.
                 umma_commit(drain);
-                mbar_wait(drain, 0, abort_flag, p.status, DEV_TIMEOUT_MMA, true);
+                mbar_wait(drain, 0, abort_flag, p.status, DEV_TIMEOUT_MMA, p.wait_ns, true);
             }
         }
         __syncwarp();
@@ -549,7 +555,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         for (int t = blockIdx.x; t < total; t += gridDim.x) {
             const int nt = t % p.n_tiles, mt = t / p.n_tiles;
             int ok = 1;
-            if (lane == 0) ok = mbar_wait(&tfull[acc], acc_phase, abort_flag, p.status, DEV_TIMEOUT_EPILOGUE);
+            if (lane == 0) ok = mbar_wait(&tfull[acc], acc_phase, abort_flag, p.status, DEV_TIMEOUT_EPILOGUE, p.wait_ns);
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) break;
             tc_fence_after();
@@ -686,6 +692,17 @@ __device__ __forceinline__ void umma_commit_pair_own(uint64_t* bar) {
                  : "memory");
 }
 
+// Cancels `bytes` of the current phase's expected transaction count.
+__device__ __forceinline__ void mbar_complete_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ uint32_t ld_shared_cluster_u32(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
 }
@@ -711,6 +728,7 @@ __global__ void __maxnreg__(128)
     uint64_t* drain = tempty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    uint32_t* nfill = reinterpret_cast<uint32_t*>(tmem_slot + 2);  // loads issued per stage (this CTA)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = cluster_rank();
@@ -727,6 +745,7 @@ __global__ void __maxnreg__(128)
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
+        for (int st = 0; st < STAGES2; ++st) nfill[st] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
@@ -747,14 +766,14 @@ __global__ void __maxnreg__(128)
         if (lane == 0) {
             // ------------------------------------------------ TMA producer (both CTAs)
             int stage = 0;
-            uint32_t phase = 0, filled = 0, filled_phase = 0;
+            uint32_t phase = 0;
             bool ok = true;
             const uint32_t tx_pair = 2u * (2u * A_BYTES + 2u * (uint32_t)half * ROW_BYTES);
             for (int t = pair; t < total && ok; t += npairs) {
                 const int nt = t % p.n_tiles, mt = t / p.n_tiles;
                 if (p.sym && !sym_tile_live(p, mt, nt)) continue;
                 for (int kc = 0; kc < p.k_chunks; ++kc) {
-                    if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_PRODUCER)) {
+                    if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_PRODUCER, p.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -779,16 +798,9 @@ __global__ void __maxnreg__(128)
                                    (p.b_group ? (int)(((int64_t)mt * 256 / p.b_group) * p.b_group_ld) : 0);
                     tma_load_2d_pair(st + 2 * A_BYTES, &mB_hi, fb, x, by);
                     tma_load_2d_pair(st + 2 * A_BYTES + B2_BYTES, &mB_lo, fb, x, by);
-                    filled |= 1u << stage;
-                    filled_phase = (filled_phase & ~(1u << stage)) | (phase << stage);
+                    ++nfill[stage];
                     if (++stage == STAGES2) stage = 0, phase ^= 1;
                 }
-            }
-            if ((!ok || *abort_flag) && leader) {
-                for (int s = 0; s < STAGES2; ++s)
-                    if (filled & (1u << s))
-                        mbar_wait(&full[s], (filled_phase >> s) & 1u, abort_flag, p.status, DEV_TIMEOUT_PRODUCER,
-                                  true);
             }
         }
         __syncwarp();
@@ -804,14 +816,14 @@ __global__ void __maxnreg__(128)
             bool ok = true, issued = false;
             for (int t = pair; t < total && ok; t += npairs) {
                 if (p.sym && !sym_tile_live(p, t / p.n_tiles, t % p.n_tiles)) continue;
-                if (!mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_MMA)) {
+                if (!mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.status, DEV_TIMEOUT_MMA, p.wait_ns)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
                 const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN_MAX);
                 for (int kc = 0; kc < p.k_chunks; ++kc) {
-                    if (!mbar_wait(&full[stage], phase, abort_flag, p.status, DEV_TIMEOUT_MMA)) {
+                    if (!mbar_wait(&full[stage], phase, abort_flag, p.status, DEV_TIMEOUT_MMA, p.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -840,7 +852,7 @@ __global__ void __maxnreg__(128)
             }
             if ((!ok || *abort_flag) && issued) {
                 umma_commit_pair_own(drain);
-                mbar_wait(drain, 0, abort_flag, p.status, DEV_TIMEOUT_MMA, true);
+                mbar_wait(drain, 0, abort_flag, p.status, DEV_TIMEOUT_MMA, p.wait_ns, true);
             }
         }
         __syncwarp();
@@ -855,7 +867,7 @@ __global__ void __maxnreg__(128)
             const int nt = t % p.n_tiles, mt = t / p.n_tiles;
             if (p.sym && !sym_tile_live(p, mt, nt)) continue;
             int ok = 1;
-            if (lane == 0) ok = mbar_wait(&tfull[acc], acc_phase, abort_flag, p.status, DEV_TIMEOUT_EPILOGUE);
+            if (lane == 0) ok = mbar_wait(&tfull[acc], acc_phase, abort_flag, p.status, DEV_TIMEOUT_EPILOGUE, p.wait_ns);
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) break;
             tc_fence_after();
@@ -1017,6 +1029,27 @@ __global__ void __maxnreg__(128)
     }
 
     tc_fence_before();
+    cluster_sync_all();
+    // Every operand load either CTA issued completes on the leader's full
+    // barriers, and after an abort the two producers may have stopped one load
+    // apart on a stage (each needs the other's previous load of the stage
+    // consumed before issuing the next, so the counts differ by at most one).
+    // The leader settles the last phase of every stage — arming a phase only
+    // the peer loaded, or cancelling the peer's half of a phase only the leader
+    // loaded — and waits for it (DRAIN_NS), so that no load is in flight when
+    // either CTA exits.  In a run without abort the counts agree and every
+    // phase has long completed.
+    if (leader && threadIdx.x == 0) {
+        const uint32_t peer_bytes = 2u * A_BYTES + 2u * (uint32_t)half * ROW_BYTES;
+        for (int s = 0; s < STAGES2; ++s) {
+            const uint32_t L = nfill[s], P = ld_shared_cluster_u32(mapa_shared(saddr(&nfill[s]), 1));
+            if (L == 0 && P == 0) continue;
+            if (P == L + 1) mbar_expect_tx(&full[s], peer_bytes);
+            else if (L == P + 1) mbar_complete_tx(&full[s], peer_bytes);
+            const uint32_t last = (L > P ? L : P) - 1;
+            mbar_wait(&full[s], last & 1u, abort_flag, p.status, DEV_TIMEOUT_PRODUCER, p.wait_ns, true);
+        }
+    }
     cluster_sync_all();
     if (warp == 1) {
         tc_fence_after();
@@ -1209,6 +1242,7 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
     p.d_hi = D_hi;
     p.d_lo = D_lo;
     p.status = h->d_status;
+    p.wait_ns = h->wait_limit_ns;
     CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
     // B rows: the modes, or (grouped) every group's modes one after another
     const int64_t b_rows = mp.b_group ? mp.b_group_ld * ((mp.R + mp.b_group - 1) / mp.b_group) : mp.M;

@@ -78,6 +78,14 @@ int fcb200_trim(fcb200_handle h);
  * bounded wait (FCB_ERR_TIMEOUT) since the last check. */
 int fcb200_synchronize(fcb200_handle h, void* stream);
 
+/* Limit, in nanoseconds, of every mbarrier wait in the tensor-core kernels of
+ * this handle (no counterpart in the reference).  A wait that runs out sets
+ * the device status word, the kernel drains the copies and MMAs it issued
+ * (those drains always get 2 s), frees its tensor memory and returns, and the
+ * next fcb200_synchronize reports FCB_ERR_TIMEOUT; the handle stays usable.
+ * limit_ns <= 0 restores the default of 2 s. */
+int fcb200_set_wait_limit(fcb200_handle h, int64_t limit_ns);
+
 /*
  * Dense third-order IFCs of a pair Lennard-Jones system with the analytical
  * calculator.  Replaces

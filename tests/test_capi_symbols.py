@@ -62,3 +62,4 @@ def test_null_handle_is_an_argument_error(fcb):
     assert L.fcb200_third_order_lj(None, None, 0, None, 0, 0, 0, 0, None, None, None, 0, None) == _lib.FCB_ERR_ARG
     assert L.fcb200_mcc3(None, None, None, 0, 0, 0, 0, 0, 0, 0, 0, None, None) == _lib.FCB_ERR_ARG
     assert L.fcb200_destroy(None) == _lib.FCB_OK
+    assert L.fcb200_set_wait_limit(None, 1) == _lib.FCB_ERR_ARG
