@@ -1,0 +1,189 @@
+"""The benchmark configurations that the other GPU tests do not reach, each
+against the oracle:
+
+* the 400-atom size class of the batching configuration (FCC 5×5×4, n = 1200,
+  a 13.8 GB FP64 Ψ): the FP64 Ψ of fcb200_snapshot_lj bit-exact against the
+  oracle slab by slab (the dense tensor is never held whole on the host), and
+  K3 over two mode windows against the oracle's FP64 contraction, in BF16×3
+  and TF32×3;
+* one batch of all three size classes (108, 256 and 400 atoms), replayed as a
+  CUDA graph, every K3 against the oracle;
+* the plain configuration: the perfect 256-atom lattice, FP64 IFC2/IFC3 and the
+  FP32 mass-weighted operand bit-exact, then FP32 mcc3 with block_size = 256
+  (27 blocks, host result; src/mcc.jl:89-120) against the FP64 oracle;
+* the three-body configuration: Stillinger-Weber diamond Si 3×3×3 (216 atoms,
+  displaced 0.03 Å) through fcb200_snapshot_sw over all 648 modes, FP32,
+  BF16×3 and TF32×3, against oracle third_order_sw → mass weighting → FP64
+  contraction.
+
+Tolerances: FP64 LJ Ψ bit-exact (np.array_equal); SW Ψ 1e-12 max-abs; K3
+max|ΔK|/max|K_ref| ≤ 1e-5 and RMS(ΔK)/RMS(K_ref) ≤ 1e-5 over the compared
+entries (the whole K3, or each window), with K_ref the FP64 contraction of the
+FP32-rounded mass-weighted oracle Ψ and the same FP32 φ.
+"""
+import numpy as np
+import pytest
+
+from conftest import AR, fcc_system
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+# (first, second, third) mode windows of the 400-atom K3: the lowest modes, and
+# a window mixing the lowest, middle and highest modes
+WINDOWS = [((0, 128), (0, 128), (0, 128)), ((0, 128), (536, 664), (1072, 1200))]
+
+
+def _err(k, ref):
+    d = np.asarray(k, dtype=np.float64) - ref
+    return float(np.max(np.abs(d)) / np.max(np.abs(ref))), float(np.sqrt(np.mean(d ** 2)) / np.sqrt(np.mean(ref ** 2)))
+
+
+def _lj(fcb):
+    return fcb.LJ(AR["sigma"], AR["eps"], AR["r_cut"]), fcb.AnalyticalCalculator(1e-12, AR["r_cut"])
+
+
+def _phi32(oracle, s):
+    ifc2 = oracle.second_order_lj(s.positions, s.box_sizes, AR["sigma"], AR["eps"], AR["r_cut"], 1e-12)
+    _, phi = oracle.get_modes(oracle.dynamical_matrix(ifc2, s.masses))
+    return np.asfortranarray(phi.astype(np.float32))
+
+
+def _full_ref(oracle, s, phi32):
+    psi = oracle.third_order_lj(s.positions, s.box_sizes, AR["sigma"], AR["eps"], AR["r_cut"], 1e-12)
+    mw = oracle.mass_weight_third_order(psi, s.masses).astype(np.float32)
+    del psi
+    return oracle.mcc3(mw.astype(np.float64), phi32.astype(np.float64))
+
+
+@pytest.fixture(scope="module")
+def cell400(fcb, oracle):
+    # the largest size class at the largest displacement of the batching configuration
+    s = fcc_system((5, 5, 4), 0.08, 4004)
+    return {"s": s, "phi32": _phi32(oracle, s), "ref": None}
+
+
+def _windows_ref(oracle, c, psi_dev=None):
+    """The oracle's K3 windows of the 400-atom cell (computed once); with
+    psi_dev, every slab of the GPU's FP64 Ψ is compared with the oracle's."""
+    bad = []
+
+    def on_slab(j0, j1, slab):
+        if psi_dev is not None and not np.array_equal(psi_dev[:, j0:j1, :].cpu().numpy(), slab):
+            bad.append((j0, j1))
+
+    if c["ref"] is None or psi_dev is not None:
+        s = c["s"]
+        win = [tuple(np.arange(a, b) for a, b in w) for w in WINDOWS]
+        c["ref"] = oracle.mcc3_windows_lj(s.positions, s.box_sizes, AR["sigma"], AR["eps"], AR["r_cut"], 1e-12,
+                                          s.masses, c["phi32"].astype(np.float64), win, on_slab=on_slab)
+    return c["ref"], bad
+
+
+def _check_windows(k3_dev, ref, label):
+    for ((a0, a1), (b0, b1), (c0, c1)), r in zip(WINDOWS, ref):
+        mx, rms = _err(k3_dev[a0:a1, b0:b1, c0:c1].cpu().numpy(), r)
+        assert mx <= TOL and rms <= TOL, (label, (a0, b0, c0), mx, rms)
+
+
+def test_snapshot_400_atoms_vs_oracle(fcb, oracle, cuda_device, cell400):
+    import torch
+    from fcb200.arrays import julia_empty
+    s, phi32 = cell400["s"], cell400["phi32"]
+    pot, calc = _lj(fcb)
+    n = 3 * s.n_atoms
+    d_phi = torch.from_numpy(phi32).to(cuda_device)
+    psi = julia_empty((n, n, n), np.float64, "cuda")
+    k3 = julia_empty((n, n, n), np.float32, "cuda")
+    fcb.snapshot_lj(s, pot, calc, d_phi, precision="bf16x3", psi_out=psi, k3_out=k3)
+    torch.cuda.synchronize()
+    ref, bad = _windows_ref(oracle, cell400, psi)
+    assert not bad, f"FP64 Ψ differs from the oracle in the column slabs {bad}"
+    del psi
+    torch.cuda.empty_cache()
+    _check_windows(k3, ref, "bf16x3")
+    k3.fill_(np.nan)
+    fcb.snapshot_lj(s, pot, calc, d_phi, precision="tf32x3", k3_out=k3)
+    torch.cuda.synchronize()
+    _check_windows(k3, ref, "tf32x3")
+
+
+def test_batch_three_sizes_vs_oracle(fcb, oracle, cuda_device, cell400):
+    import torch
+    from fcb200.batch import SnapshotBatch
+    pot, calc = _lj(fcb)
+    s108, s256 = fcc_system((3, 3, 3), 0.03, 108), fcc_system((4, 4, 4), 0.05, 256)
+    phis = [_phi32(oracle, s108), _phi32(oracle, s256), cell400["phi32"]]
+    b = SnapshotBatch("bf16x3")
+    outs = [b.add(s, pot, calc, p) for s, p in zip((s108, s256, cell400["s"]), phis)]
+    b.run()                      # eager: sizes the lanes' scratch
+    b.run()                      # captured as one graph and launched
+    for o in outs:
+        o.fill_(np.nan)
+    b.run()                      # graph replay alone must rewrite every K3
+    torch.cuda.synchronize()
+    info = b.info()
+    assert info["snapshots"] == 3
+    for s, p, o in zip((s108, s256), phis[:2], outs[:2]):
+        mx, rms = _err(o.cpu().numpy(), _full_ref(oracle, s, p))
+        assert mx <= TOL and rms <= TOL, (s.n_atoms, mx, rms)
+    ref, _ = _windows_ref(oracle, cell400)
+    _check_windows(outs[2], ref, "batch 400 atoms")
+    b.close()
+
+
+def test_config1_perfect_lattice_fp32_blocked(fcb, oracle, cuda_device):
+    import torch
+    from fcb200.arrays import julia_empty
+    s = fcc_system((4, 4, 4))                              # perfect lattice
+    pot, calc = _lj(fcb)
+    n = 3 * s.n_atoms
+    psi = julia_empty((n, n, n), np.float64, "cuda")
+    psi32 = julia_empty((n, n, n), np.float32, "cuda")
+    fcb.third_order_(psi, s, pot, calc, psi32_mw=psi32)
+    torch.cuda.synchronize()
+    ref_psi = oracle.third_order_lj(s.positions, s.box_sizes, pot.sigma, pot.eps, pot.r_cut, 1e-12)
+    assert np.array_equal(psi.cpu().numpy(), ref_psi)
+    del psi
+    mw32 = oracle.mass_weight_third_order(ref_psi, s.masses).astype(np.float32)
+    del ref_psi
+    assert np.array_equal(psi32.cpu().numpy(), mw32)
+    dyn = fcb.dynamical_matrix(s, pot, calc, device="cuda")
+    ref_dyn = oracle.dynamical_matrix(
+        oracle.second_order_lj(s.positions, s.box_sizes, pot.sigma, pot.eps, pot.r_cut, 1e-12), s.masses)
+    assert np.max(np.abs(dyn.values.cpu().numpy() - ref_dyn)) <= 1e-12 * np.max(np.abs(ref_dyn))
+    _, _, phi = fcb.get_modes(dyn, 3, phi32=True)          # FP32 eigenvectors, on the device
+    k3 = fcb.mcc3(psi32, phi, 256, precision="fp32")       # 27 blocks, host result
+    assert isinstance(k3, np.ndarray) and k3.shape == (n, n, n)
+    del psi32
+    ref = oracle.mcc3(mw32.astype(np.float64), phi.cpu().numpy().astype(np.float64))
+    mx, rms = _err(k3, ref)
+    assert mx <= TOL and rms <= TOL, (mx, rms)
+
+
+@pytest.fixture(scope="module")
+def sw216(fcb, oracle):
+    s = fcb.displaced(fcb.Diamond(5.43, "Si", (3, 3, 3)), 0.03, 216)
+    pot = fcb.StillingerWeberSilicon()
+    calc = fcb.AutoDiffCalculator(1e-12, pot.r_cut)
+    psi = oracle.third_order_sw(s.positions, s.box_sizes, pot.r_cut, 1e-12)
+    mw32 = oracle.mass_weight_third_order(psi.copy(order="F"), s.masses).astype(np.float32)
+    ifc2 = oracle.second_order_sw(s.positions, s.box_sizes, pot.r_cut, 1e-12)
+    _, phi = oracle.get_modes(oracle.dynamical_matrix(ifc2, s.masses))
+    phi32 = np.asfortranarray(phi.astype(np.float32))
+    ref = oracle.mcc3(mw32.astype(np.float64), phi32.astype(np.float64))
+    return s, pot, calc, psi, phi32, ref
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3", "tf32x3"])
+def test_sw_snapshot_216_atoms_vs_oracle(fcb, cuda_device, sw216, precision):
+    import torch
+    from fcb200.arrays import julia_empty
+    s, pot, calc, psi_ref, phi32, ref = sw216
+    n = 3 * s.n_atoms
+    psi = julia_empty((n, n, n), np.float64, "cuda")
+    _, k3 = fcb.snapshot_lj(s, pot, calc, torch.from_numpy(phi32).to(cuda_device), precision=precision,
+                            psi_out=psi)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(psi.cpu().numpy() - psi_ref)) <= 1e-12
+    mx, rms = _err(k3.cpu().numpy(), ref)
+    assert mx <= TOL and rms <= TOL, (precision, mx, rms)
