@@ -431,6 +431,19 @@ int fcb200_batch_info(fcb200_batch_t b, int64_t* n_snapshots, int64_t* lanes, in
     return FCB_OK;
 }
 
+int fcb200_batch_lane(fcb200_batch_t b, int64_t index, int64_t* lane) {
+    if (!b || !lane || index < 0 || index >= (int64_t)b->snaps.size()) return set_error(FCB_ERR_ARG, "bad argument");
+    if (b->dirty || b->plan.empty())
+        return set_error(FCB_ERR_ARG, "the batch has no plan yet: fcb200_batch_run makes it");
+    for (size_t l = 0; l < b->plan.size(); ++l)
+        for (int i : b->plan[l])
+            if (i == index) {
+                *lane = (int64_t)l;
+                return FCB_OK;
+            }
+    return set_error(FCB_ERR_ARG, "snapshot not in the plan");
+}
+
 int fcb200_batch_destroy(fcb200_batch_t b) {
     if (!b) return FCB_OK;
     cudaSetDevice(b->h->device);

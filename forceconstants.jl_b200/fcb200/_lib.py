@@ -69,6 +69,7 @@ SIGNATURES = {
     "fcb200_batch_run": (_I, [_P, _P]),
     "fcb200_batch_info": (_I, [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64),
                                ctypes.POINTER(ctypes.c_size_t)]),
+    "fcb200_batch_lane": (_I, [_P, _I64, ctypes.POINTER(_I64)]),
     "fcb200_batch_destroy": (_I, [_P]),
     "fcb200_mcc3_adjoint_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _P, _P, _I64, _P, _I, _P,
                                     ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D), _P]),

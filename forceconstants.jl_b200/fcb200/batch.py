@@ -47,6 +47,12 @@ class SnapshotBatch:
                                                 ctypes.byref(d)))
         return {"snapshots": a.value, "lanes": b.value, "graph_nodes": c.value, "scratch_bytes": d.value}
 
+    def lane(self, index: int) -> int:
+        """Lane of snapshot ``index`` in the current plan (after the first run)."""
+        out = ctypes.c_int64()
+        _lib.check(_lib.lib().fcb200_batch_lane(self._b, int(index), ctypes.byref(out)))
+        return out.value
+
     def close(self):
         if self._b:
             _lib.lib().fcb200_batch_destroy(self._b)

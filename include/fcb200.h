@@ -322,6 +322,12 @@ int fcb200_batch_set_positions(fcb200_batch_t b, int64_t index, const double* po
 int fcb200_batch_run(fcb200_batch_t b, void* stream);
 int fcb200_batch_info(fcb200_batch_t b, int64_t* n_snapshots, int64_t* lanes, int64_t* graph_nodes,
                       size_t* scratch_bytes);
+/* The lane that runs snapshot `index` in the batch's current plan (made by the
+ * first fcb200_batch_run after snapshots were added or re-planned;
+ * FCB_ERR_ARG before that).  A lane runs its snapshots one after another, so
+ * snapshots of one lane may share a K3 output buffer; snapshots of different
+ * lanes run concurrently and must not. */
+int fcb200_batch_lane(fcb200_batch_t b, int64_t index, int64_t* lane);
 int fcb200_batch_destroy(fcb200_batch_t b);
 
 /*
