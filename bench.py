@@ -8,7 +8,7 @@ assembly (+ASR, tol) with the fused mass-weighted split operand, then mcc3 over
 all 768 modes (three mode products), K3 in FP32.  Inputs are synthetic (seeded).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3|tf32x3|fp32]
-                    [--impl ours|reference]
+                    [--impl ours|reference] [--out-dir DIR]
 
 Prints one JSON line (rank 0).  Time-like metric: value = seconds per snapshot
 for the whole job (max over ranks of the device time ÷ all snapshots).  N > 1
@@ -24,6 +24,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -109,10 +110,10 @@ class Clocks:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, out_dir: str):
         self.idx = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        self.path = os.path.join(out_dir, f"clocks_bench_{os.getpid()}.csv")
 
     def start(self):
         try:
@@ -158,7 +159,7 @@ def build_workload(fcb, device):
     pot = fcb.LJ(SIGMA, EPS, R_CUT)
     calc = fcb.AnalyticalCalculator(TOL, R_CUT)
     dyn = fcb.dynamical_matrix(s, pot, calc)               # on the GPU (fcb200_second_order_lj)
-    _, phi = fcb.get_modes(dyn)                             # host LAPACK, as the reference (dynmat.jl:125)
+    _, phi = fcb.get_modes(dyn)                             # on the GPU (fcb200_get_modes, cuSOLVER syevd)
     phi32 = np.asfortranarray(phi.astype(np.float32))
     return s, pot, calc, phi32
 
@@ -193,10 +194,11 @@ def err_vs(k3_dev, ref):
             "rms_rel": float(torch.sqrt((d * d).mean()) / torch.sqrt((ref * ref).mean()))}
 
 
-def cpu_baseline(threads=None):
-    """The oracle (CPU restatement of the reference path) on the host cores:
-    full 256-atom third_order (all threads) + serial mass weighting + FP32 cast
-    measured; the FP64 mcc3 timed on 1/16 of mode product 1 and scaled by flops."""
+def cpu_baseline(phi32, threads=None):
+    """The oracle (CPU restatement of the reference path) on the host cores, one
+    whole snapshot measured: 256-atom third_order (all threads), serial mass
+    weighting, the FP32 cast, and the FP64 mcc3 over all 768 modes (three mode
+    products, numpy BLAS on all threads) with the same φ as the GPU step."""
     from oracle import oracle as O
     import fcb200 as fcb
     if threads:
@@ -211,55 +213,60 @@ def cpu_baseline(threads=None):
     f32 = np.empty(n ** 3, np.float32)
     O.lib().oracle_cast_f32(O._pd(psi.reshape(-1, order="F")), f32.ctypes.data_as(O._PF), n ** 3)
     t3 = time.perf_counter()
-    phi = np.linalg.qr(np.random.default_rng(0).normal(size=(n, n)))[0]
-    a = psi.reshape(n, n * n, order="F")
-    frac = 16
+    del psi
+    psi32 = f32.reshape((n, n, n), order="F")
     t4 = time.perf_counter()
-    _ = phi.T @ a[:, : n * n // frac]
+    _ = O.mcc3(psi32, phi32)
     t5 = time.perf_counter()
-    mcc3_est = (t5 - t4) * frac * 3
-    total = (t1 - t0) + (t2 - t1) + (t3 - t2) + mcc3_est
+    total = t5 - t0 - (t4 - t3)
     return {"value": total, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-            "sample": (f"oracle on the full 256-atom cell: third_order {t1 - t0:.2f}s ({O.num_threads()} threads) + "
-                       f"serial mass_weight {t2 - t1:.2f}s + cast {t3 - t2:.2f}s measured; FP64 mcc3 "
-                       f"{mcc3_est:.2f}s scaled from 1/{frac} of mode product 1 (numpy BLAS) x3 products")}
+            "sample": (f"one whole 256-atom snapshot by the oracle, all measured: third_order {t1 - t0:.2f}s "
+                       f"({O.num_threads()} threads) + serial mass_weight {t2 - t1:.2f}s + cast {t3 - t2:.2f}s + "
+                       f"FP64 mcc3 over 768 modes {t5 - t4:.2f}s (numpy BLAS)")}
 
 
-def batch_config(fcb, precision, device, reps=3):
+def batch_config(fcb, precision, device, out_dir, reps=3):
     """The batching configuration: 48 LJ argon snapshots of uneven size (16 each
     of FCC 3x3x3 = 108, 4x4x4 = 256 and 5x5x4 = 400 atoms), displacement std
     drawn from U(0.03, 0.08) A per snapshot (seeded), through assembly, mass
     weighting and full-mode mcc3 as one CUDA-graph launch per batch.  phi per
     size class from the perfect lattice (the modes of the reference structure,
-    shared by its snapshots).  Each size class writes its K3 into one device
-    buffer (results consumed in place), so scratch is budgeted for one lane."""
+    shared by its snapshots).  The scratch budget admits two lanes; every lane
+    has its own K3 buffer per size class (snapshots of one lane run one after
+    another, fcb200_batch_lane), and after the timed runs the last K3 of each
+    size class is checked bit for bit against the single-snapshot path."""
     import torch
     from fcb200.batch import SnapshotBatch, autotune_mcc3
     rng = np.random.default_rng(4242)
     pot = fcb.LJ(SIGMA, EPS, R_CUT)
     calc = fcb.AnalyticalCalculator(TOL, R_CUT)
     classes = [(3, 3, 3), (4, 4, 4), (5, 5, 4)]
+    lanes = 2
     t0 = time.perf_counter()
-    cache = os.path.join(ROOT, "gpurun_out", "autotune_mcc3.json")
-    os.makedirs(os.path.dirname(cache), exist_ok=True)
+    cache = os.path.join(out_dir, "autotune_mcc3.json")
     for c in classes:
         autotune_mcc3(12 * c[0] * c[1] * c[2], precision, cache)
     tune_s = time.perf_counter() - t0
     b = SnapshotBatch(precision, hbm_budget_bytes=int(1.2 * (2 * 2 * 1200 * (3 * 1200 ** 2 + 1200) + 40e6)))
-    outs = {}
+    outs, members, phis = {}, [], {}
     for c in classes:
         base = fcb.FCC(A_LAT, "Ar", c)
         dyn = fcb.dynamical_matrix(base, pot, calc)
         _, phi = fcb.get_modes(dyn)
-        phi32 = np.asfortranarray(phi.astype(np.float32))
+        phis[c] = np.asfortranarray(phi.astype(np.float32))
         n = 3 * base.n_atoms
-        outs[c] = julia_tensor((n, n, n), np.float32, device)
-        for _ in range(16):
+        outs[c] = [julia_tensor((n, n, n), np.float32, device) for _ in range(lanes)]
+        for j in range(16):
             s = fcb.displaced(base, float(rng.uniform(0.03, 0.08)), int(rng.integers(1 << 30)))
-            b.add(s, pot, calc, phi32, k3_out=outs[c])
+            b.add(s, pot, calc, phis[c], k3_out=outs[c][j % lanes])
+            members.append((c, j % lanes, s))
     stream = torch.cuda.current_stream()
     sp = int(stream.cuda_stream)
-    b.run(sp)                 # eager: sizes the lane scratch
+    b.run(sp)                 # eager: makes the plan and sizes the lane scratch
+    info = b.info()
+    for i, (c, slot, _) in enumerate(members):
+        if info["lanes"] != lanes or b.lane(i) != slot:
+            raise RuntimeError("the batch plan does not put the snapshots that share a K3 buffer in one lane")
     b.run(sp)                 # capture + first graph launch
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -270,14 +277,167 @@ def batch_config(fcb, precision, device, reps=3):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
     info = b.info()
+    # the last snapshot of each size class in lane 0 wrote that class's lane-0 buffer last
+    checked = {}
+    for c in classes:
+        last = [s for (cc, slot, s) in members if cc == c and slot == 0][-1]
+        _, k = fcb.snapshot_lj(last, pot, calc, torch.from_numpy(phis[c]).to(device), precision=precision)
+        torch.cuda.synchronize()
+        checked[f"{3 * last.n_atoms}"] = bool(torch.equal(k, outs[c][0]))
     b.close()
     del outs
     torch.cuda.empty_cache()
+    if not all(checked.values()):
+        raise RuntimeError(f"batch K3 differs from the single-snapshot path: {checked}")
     return {"snapshots": info["snapshots"], "s_per_batch": ms / 1e3, "snapshots_per_s": info["snapshots"] / (ms / 1e3),
             "s_per_snapshot": ms / 1e3 / info["snapshots"], "graph_launches_per_batch": 1,
             "graph_nodes": info["graph_nodes"], "lanes": info["lanes"], "scratch_bytes": info["scratch_bytes"],
             "autotune_s": round(tune_s, 2), "precision": precision,
+            "k3_buffers": "one per lane and size class (snapshots of a lane run in sequence)",
+            "bitwise_equal_to_single_snapshot_path": checked,
             "workload": "48 LJ snapshots: 16x108, 16x256, 16x400 atoms, std U(0.03,0.08) A, full-mode mcc3"}
+
+
+def gemm_peaks(device, reps=10):
+    """Dense GEMM throughput of this GPU, the roofline denominators of the FP32
+    and TF32x3 forms (MEASURED_PEAKS.json holds the HBM copy and BF16 GEMM
+    figures only): torch.matmul (cuBLAS) of 8192 x 8192 FP32 matrices with
+    TF32 off (FFMA) and on (tensor cores), CUDA events around `reps` calls
+    after 3 warm-up calls (a burst, like MEASURED_PEAKS.json's bf16_tflops)."""
+    import torch
+    n = 8192
+    a, b = torch.randn(n, n, device=device), torch.randn(n, n, device=device)
+    c = torch.empty(n, n, device=device)
+    prev = torch.backends.cuda.matmul.allow_tf32
+    out = {}
+    try:
+        for name, tf32 in (("fp32_tflops", False), ("tf32_tflops", True)):
+            torch.backends.cuda.matmul.allow_tf32 = tf32
+            for _ in range(3):
+                torch.matmul(a, b, out=c)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                torch.matmul(a, b, out=c)
+            e1.record()
+            torch.cuda.synchronize()
+            out[name] = round(2.0 * n ** 3 * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12, 1)
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b, c
+    torch.cuda.empty_cache()
+    out["method"] = f"torch.matmul FP32 {n}^3, TF32 off / on, {reps} calls after 3 warm-up, CUDA events"
+    return out
+
+
+def timed(fn, stream, reps):
+    """Mean device time (s) of fn() over `reps` calls, CUDA events on `stream`."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps / 1e3
+
+
+def sw_snapshot_config(fcb, device, stream, reps=3):
+    """The three-body configuration: Stillinger-Weber diamond Si 3x3x3 (216
+    atoms, n = 648), displaced std 0.03 A (seed 216), φ from its dynamical
+    matrix (on the GPU); one step = fcb200_snapshot_sw (FP64 SW IFC3 with ASR,
+    the mass-weighted operand, mcc3 over all 648 modes)."""
+    import torch
+    s = fcb.displaced(fcb.Diamond(5.43, "Si", (3, 3, 3)), 0.03, 216)
+    pot = fcb.StillingerWeberSilicon()
+    calc = fcb.AutoDiffCalculator(TOL, pot.r_cut)
+    dyn = fcb.dynamical_matrix(s, pot, calc, device=device)
+    _, _, phi = fcb.get_modes(dyn, 3, phi32=True)
+    n = 3 * s.n_atoms
+    psi = julia_tensor((n, n, n), np.float64, device)
+    k3 = julia_tensor((n, n, n), np.float32, device)
+    sp = int(stream.cuda_stream)
+    out = {"workload": "SW diamond Si 3x3x3 (216 atoms, n=648), std 0.03 A seed 216, all 648 modes, FP64 Psi written"}
+    ref = None
+    for precision in ("bf16x3", "tf32x3", "fp32"):
+        def step():
+            fcb.snapshot_lj(s, pot, calc, phi, precision=precision, psi_out=psi, k3_out=k3, stream=sp)
+        step()
+        torch.cuda.synchronize()
+        if ref is None:
+            ref = fp64_reference_k3(psi, s.masses, phi.cpu().numpy())
+        out[precision] = {"s_per_snapshot": timed(step, stream, reps), "error_vs_fp64": err_vs(k3, ref)}
+    del ref, psi, k3
+    torch.cuda.empty_cache()
+    return out
+
+
+def adjoint_config(fcb, device, stream, s, pot, calc, reps=3):
+    """The differentiation configuration: the 256-atom displaced cell, φ frozen,
+    W ~ N(0,1) over the first 256 modes (seeded); one call of
+    fcb200_mcc3_adjoint_lj gives dL/dpositions (768), dL/dsigma, dL/deps and L
+    (device inputs; it synchronises once to read the scalars)."""
+    import torch
+    from fcb200.adjoint import mcc3_adjoint_lj
+    from fcb200.arrays import as_julia
+    M = 256
+    dyn = fcb.dynamical_matrix(s, pot, calc, device=device)
+    _, _, phi = fcb.get_modes(dyn, 3, phi32=True)
+    W = as_julia(torch.from_numpy(np.random.default_rng(2025).normal(size=(M, M, M)).astype(np.float32)).to(device),
+                 np.float32)
+    out = {"workload": "256-atom LJ cell (std 0.05 A seed 1234), W over modes 0..255, grads of L = sum W*K3",
+           "checked": "tests/test_gpu_adjoint.py: all 768 position components, sigma and eps within 1e-6 of "
+                      "central differences (h = 1e-5 A) with G in FP64"}
+    for precision in ("fp64", "tf32x3", "fp32"):
+        def call():
+            mcc3_adjoint_lj(s, pot, calc, phi, W, precision=precision)
+        call()
+        out[precision] = {"s_per_call": timed(call, stream, reps)}
+    del W
+    torch.cuda.empty_cache()
+    return out
+
+
+def config1(fcb, device, stream, reps=3):
+    """The plain configuration: the perfect 256-atom lattice, FP64 IFC3 with the
+    fused FP32 mass-weighted copy, φ = FP32 eigenvectors of the dynamical
+    matrix (on the GPU), then FP32 mcc3 with block_size = 256 (27 blocks, the
+    result in host memory as mcc.jl:89-120 returns it)."""
+    import torch
+    from fcb200 import _lib
+    s = fcb.FCC(A_LAT, "Ar", CELLS)
+    pot = fcb.LJ(SIGMA, EPS, R_CUT)
+    calc = fcb.AnalyticalCalculator(TOL, R_CUT)
+    n = 3 * s.n_atoms
+    psi = julia_tensor((n, n, n), np.float64, device)
+    psi32 = julia_tensor((n, n, n), np.float32, device)
+    sp = int(stream.cuda_stream)
+
+    def assemble():
+        fcb.third_order_(psi, s, pot, calc, psi32_mw=psi32)
+
+    asm = timed(assemble, stream, reps)
+    dyn = fcb.dynamical_matrix(s, pot, calc, device=device)
+    _, _, phi = fcb.get_modes(dyn, 3, phi32=True)
+    k3_h = torch.empty(n ** 3, dtype=torch.float32).pin_memory()
+    L = _lib.lib()
+    h = _lib.handle(torch.device(device).index or 0)
+
+    def blocked():
+        _lib.check(L.fcb200_mcc3_blocked(h, int(psi32.data_ptr()), int(phi.data_ptr()), n, 256, _lib.FCB_MCC3_FP32,
+                                         int(k3_h.data_ptr()), sp))
+
+    blocked()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        blocked()
+    blk = (time.perf_counter() - t0) / reps
+    del psi, psi32, k3_h
+    torch.cuda.empty_cache()
+    return {"workload": "perfect LJ FCC 4x4x4 (256 atoms), FP64 IFC3 + FP32 mass-weighted copy, FP32 mcc3 "
+                        "block_size 256 (27 blocks) into pinned host memory",
+            "assembly_s": asm, "mcc3_blocked_fp32_host_s": blk, "d2h_bytes": 4 * n ** 3,
+            "checked": "tests/test_gpu_configs.py::test_config1_perfect_lattice_fp32_blocked"}
 
 
 def run_reference(args, rank, world):
@@ -349,6 +509,10 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-batch", action="store_true", help="omit the 48-snapshot batch configuration")
+    ap.add_argument("--skip-extra", action="store_true",
+                    help="omit the other configurations (SW snapshot, adjoint, plain FP32 blocked) and the GEMM peaks")
+    ap.add_argument("--out-dir", default=None,
+                    help="directory for the clock samples and the autotune cache (default: a temporary directory)")
     ap.add_argument("--cells", default=None, help="FCC cells 'x,y,z' (profiling cases; default 4,4,4)")
     ap.add_argument("--minimal", action="store_true",
                     help="warm-up + timed steps only (for profiler captures of small cases)")
@@ -369,6 +533,8 @@ def main():
         return
     pg = replicas.init("nccl", timeout_s=120)
     args.warmup = max(args.warmup, 3)
+    out_dir = args.out_dir or tempfile.mkdtemp(prefix="fcb200_bench_")
+    os.makedirs(out_dir, exist_ok=True)
 
 
     import fcb200 as fcb
@@ -388,17 +554,17 @@ def main():
     k3 = julia_tensor((n, n, n), np.float32, dev)
     prec = _lib.PRECISIONS[args.precision]
 
-    def step(precision=prec, k3_ptr=None, phi_ptr=None, pos_ptr=None):
+    def step(precision=prec, k3_ptr=None, phi_ptr=None, pos_ptr=None, psi_ptr=None):
         _lib.check(L.fcb200_snapshot_lj(
             h, pos_ptr or int(d_pos.data_ptr()), s.n_atoms, int(d_box.data_ptr()), SIGMA, EPS, R_CUT, TOL,
-            int(d_m.data_ptr()), phi_ptr or int(d_phi.data_ptr()), 0, n, precision, int(psi64.data_ptr()),
+            int(d_m.data_ptr()), phi_ptr or int(d_phi.data_ptr()), 0, n, precision, psi_ptr or int(psi64.data_ptr()),
             k3_ptr or int(k3.data_ptr()), sp))
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     replicas.barrier(pg)
-    clocks = Clocks(local)
+    clocks = Clocks(local, out_dir)
     clocks.start()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -423,16 +589,19 @@ def main():
         return
 
     # ---- per-phase device times (profiled pass, same stream, outside the timed region)
-    _lib.check(L.fcb200_set_profiling(h, 1))
-    reps = 3
-    acc = np.zeros(6)
-    for _ in range(reps):
-        step()
-        out = (ctypes.c_double * 6)()
-        _lib.check(L.fcb200_phase_times(h, out, 6))
-        acc += np.array(out[:])
-    _lib.check(L.fcb200_set_profiling(h, 0))
-    phases = acc / reps
+    def profile_phases(precision, reps=3):
+        _lib.check(L.fcb200_set_profiling(h, 1))
+        acc = np.zeros(6)
+        for _ in range(reps):
+            step(precision=precision)
+            out = (ctypes.c_double * 6)()
+            _lib.check(L.fcb200_phase_times(h, out, 6))
+            acc += np.array(out[:])
+        _lib.check(L.fcb200_set_profiling(h, 0))
+        return acc / reps
+
+    phases = profile_phases(prec)
+    gemm = None if args.skip_extra else gemm_peaks(dev)
     split = args.precision != "fp32"
     if split:
         # profiled pass: the FP64 writer runs alone inside the second phase; the
@@ -448,8 +617,13 @@ def main():
     if not split:
         mp_ms = float(np.mean(phases[3:6]))
         flops_launch = 2.0 * n ** 4
-        roof = {"bound": "fp32-simt", "achieved": flops_launch / (mp_ms * 1e-3) / 1e12, "peak": None,
-                "unit": "TFLOP/s", "frac": None, "traffic": None}
+        ach = flops_launch / (mp_ms * 1e-3) / 1e12
+        pk = gemm["fp32_tflops"] if gemm else None
+        roof = {"bound": "fp32-simt", "achieved": round(ach, 2), "peak": pk, "unit": "TFLOP/s",
+                "frac": round(ach / pk, 4) if pk else None, "traffic": None,
+                "kernel": "mode_product_f32_kernel (FFMA), 3 launches/step", "flops_per_launch": flops_launch,
+                "avg_launch_ms": round(mp_ms, 4),
+                "peak_source": "measured FP32 GEMM (torch/cuBLAS, TF32 off) in this run, gemm_peaks"}
     else:
         # Dominant kernel: the 2-CTA tensor-core mode product.  In the compact form
         # (taken at 256 atoms) it is the third product, reading U2 MN-major with
@@ -466,8 +640,10 @@ def main():
             flops_launch = float(np.mean([sym_executed_flops(n * n, n, n, n), sym_executed_flops(n * n, n, n, n)]))
         # The step is milliseconds long and the timed region well under a second, so the
         # burst GEMM figure is the denominator; the sustained (power-capped) one is kept beside it.
-        pk = peaks["bf16_tflops"] if args.precision == "bf16x3" else None
-        pks = peaks["bf16_tflops_sustained"] if args.precision == "bf16x3" else None
+        if args.precision == "bf16x3":
+            pk, pks = peaks["bf16_tflops"], peaks["bf16_tflops_sustained"]
+        else:   # tf32x3: the TF32 GEMM measured in this run
+            pk, pks = (gemm["tf32_tflops"] if gemm else None), None
         ach = flops_launch / (mp_ms * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": round(ach, 2), "peak": pk, "unit": "TFLOP/s",
                 "frac": round(ach / pk, 4) if pk else None,
@@ -481,7 +657,10 @@ def main():
                            "2 launches/step (P2, P3)"),
                 "flops_per_launch": flops_launch, "avg_launch_ms": round(mp_ms, 4),
                 "useful_flops_per_step": 6.0 * n ** 4,
-                "peak_source": f"{peak_src} bf16_tflops (burst; executed tensor flops = 3x per product for the split)"}
+                "peak_source": (f"{peak_src} bf16_tflops (burst; executed tensor flops = 3x per product for the split)"
+                                if args.precision == "bf16x3" else
+                                "measured TF32 GEMM (torch/cuBLAS) in this run, gemm_peaks; executed tensor flops "
+                                "= 3x per product for the split")}
         if cs:
             p2_ms = float(phases[4])
             a2 = p2_flops / (p2_ms * 1e-3) / 1e12
@@ -516,6 +695,7 @@ def main():
     acc_err = {args.precision: err_vs(k3, ref)}
     # FP32 GPU form for the "split-BF16 vs FP32 GPU" comparison
     fp32_info = None
+    packed_info = None
     if args.precision != "fp32":
         k3f = julia_tensor((n, n, n), np.float32, dev)
         step(precision=_lib.FCB_MCC3_FP32, k3_ptr=int(k3f.data_ptr()))
@@ -530,6 +710,14 @@ def main():
         torch.cuda.synchronize()
         fp32_s = f0.elapsed_time(f1) / nf / 1e3
         fp32_info = {"s_per_snapshot": fp32_s, "speedup_split_vs_fp32": fp32_s / (ms_per_step / 1e3)}
+        # the FP32 SIMT mode product against the measured FP32 GEMM
+        fph = profile_phases(_lib.FCB_MCC3_FP32, reps=1)
+        f_ms = float(np.mean(fph[3:6]))
+        f_ach = 2.0 * n ** 4 / (f_ms * 1e-3) / 1e12
+        fp32_info["mode_product"] = {
+            "kernel": "mode_product_f32_kernel (FFMA), dense, 3 launches/step", "avg_launch_ms": round(f_ms, 4),
+            "flops_per_launch": 2.0 * n ** 4, "achieved_tflops": round(f_ach, 2),
+            "frac_of_measured_fp32_gemm": round(f_ach / gemm["fp32_tflops"], 4) if gemm else None}
         # the same precision with every mode product dense (no sparse P1, no symmetric tiles)
         dense_prec = prec | _lib.FCB_MCC3_FORCE_DENSE
         step(precision=dense_prec, k3_ptr=int(k3f.data_ptr()))
@@ -541,6 +729,21 @@ def main():
         f1.record(stream)
         torch.cuda.synchronize()
         fp32_info["dense_products_s_per_snapshot"] = f0.elapsed_time(f1) / nf / 1e3
+        fp32_info["speedup_split_vs_fp32_both_dense"] = fp32_s / fp32_info["dense_products_s_per_snapshot"]
+        if args.precision == "bf16x3" and not args.skip_extra:
+            # TF32x3 on the same step: time, error and its third product against the measured TF32 GEMM
+            tf = _lib.PRECISIONS["tf32x3"]
+            step(precision=tf, k3_ptr=int(k3f.data_ptr()))
+            torch.cuda.synchronize()
+            acc_err["tf32x3"] = err_vs(k3f, ref)
+            tf_s = timed(lambda: step(precision=tf, k3_ptr=int(k3f.data_ptr())), stream, nf)
+            tph = profile_phases(tf, reps=1)
+            t_ach = flops_launch / (float(tph[5]) * 1e-3) / 1e12 if cs else None
+            fp32_info["tf32x3"] = {
+                "s_per_snapshot": tf_s, "third_product_ms": round(float(tph[5]), 4),
+                "third_product_achieved_tflops": round(t_ach, 2) if t_ach else None,
+                "third_product_frac_of_measured_tf32_gemm": round(t_ach / gemm["tf32_tflops"], 4)
+                if (t_ach and gemm) else None}
         del k3f
     del ref
     torch.cuda.empty_cache()
@@ -564,16 +767,38 @@ def main():
                "d2h_bytes_per_step": int(k3_h.numel() * 4),
                "note": "fcb200_snapshot_lj with host positions, pinned host phi and pinned host K3; "
                        "FP64 Psi stays in device memory"}
+        # the same call also returning the FP64 Ψ to (pinned) host memory, as third_order does
+        psi_h = torch.empty(n ** 3, dtype=torch.float64).pin_memory()
+        step(k3_ptr=int(k3_h.data_ptr()), phi_ptr=int(phi_h.data_ptr()), pos_ptr=pos_h.ctypes.data,
+             psi_ptr=int(psi_h.data_ptr()))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            step(k3_ptr=int(k3_h.data_ptr()), phi_ptr=int(phi_h.data_ptr()), pos_ptr=pos_h.ctypes.data,
+                 psi_ptr=int(psi_h.data_ptr()))
+        torch.cuda.synchronize()
+        e2e["with_psi64_to_host"] = {"value": (time.perf_counter() - t0) / ne, "unit": UNIT,
+                                     "d2h_bytes_per_step": int(k3_h.numel() * 4 + psi_h.numel() * 8)}
+        del psi_h
 
     batch = None
     if not args.skip_batch:
         _lib.check(L.fcb200_trim(h))
         torch.cuda.empty_cache()
-        batch = batch_config(fcb, args.precision, dev)
+        batch = batch_config(fcb, args.precision, dev, out_dir)
+
+    extra = {}
+    if not args.skip_extra:
+        _lib.check(L.fcb200_trim(h))
+        torch.cuda.empty_cache()
+        extra["sw_snapshot"] = sw_snapshot_config(fcb, dev, stream)
+        extra["adjoint"] = adjoint_config(fcb, dev, stream, s, pot, calc)
+        extra["plain_fp32_blocked"] = config1(fcb, dev, stream)
+        extra["measured_gemm_peaks"] = gemm
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
-        cpu = cpu_baseline()
+        cpu = cpu_baseline(phi32)
 
     # split: pair, self, neighbour lists, phi split, coefficients, sparse P1, P2 with the dense
     # writer beside it (second stream), P3
@@ -596,9 +821,10 @@ def main():
                      "note": "phase_ms from a profiled pass with every kernel alone; the timed steps run the "
                              "FP64 writer on a second stream beside the last tensor-core product(s)"}
                     if split else None),
-        "error_vs_fp64": acc_err, "fp32_gpu": fp32_info, "clocks": clk, "e2e": e2e,
+        "error_vs_fp64": acc_err, "fp32_gpu": fp32_info, "packed_k3": packed_info, "clocks": clk, "e2e": e2e,
         "cpu_baseline": cpu, "batch": batch, "gpu_launches": kernels_per_step * args.steps,
     }
+    line.update(extra)
     if rank == 0:
         print(json.dumps(line), flush=True)
     replicas.finalize(pg)
