@@ -66,6 +66,24 @@ def sym_executed_flops(R, F, K, M, split=3):
     return 2.0 * 256 * bn * kpad * live * split
 
 
+def full_sym_executed_flops(Mp, M, K, split=3, packed=False):
+    """Tensor flops of the third product with full symmetry: 256-row tiles
+    (rows a + Mp·b) computed when a // 256 <= b // 256, each over every 256-wide
+    mode tile (with the packed output: a0 <= b and only the mode tiles that
+    reach s >= b), K padded to whole 64-wide chunks."""
+    n_tiles = -(-M // 256)
+    bn = 256 if M > 256 else -(-M // 16) * 16
+    kpad = -(-K // 64) * 64
+    live = 0
+    for mt in range(Mp * M // 256):
+        a0, b = (mt * 256) % Mp, (mt * 256) // Mp
+        if packed:
+            live += sum(1 for nt in range(n_tiles) if a0 <= b and min(nt * bn + bn, M) - 1 >= b)
+        elif a0 // 256 <= b // 256:
+            live += n_tiles
+    return 2.0 * 256 * bn * kpad * live * split
+
+
 def sparse_cap(pos, box, r_cut):
     """Capacity of the sparse coefficient tables, as the library sizes them for a
     single snapshot: the largest neighbourhood (atoms within r_cut by the single
@@ -633,7 +651,7 @@ def main():
         if cs:
             Mp, Kc = cs
             mp_ms = float(phases[5])
-            flops_launch = sym_executed_flops(Mp * n, Mp, n, n)
+            flops_launch = full_sym_executed_flops(Mp, n, n)
             p2_flops = inner_sym_executed_flops(n, n, Mp, Kc)
         else:
             mp_ms = float(np.mean(phases[4:6]))
@@ -651,8 +669,8 @@ def main():
                 "traffic": NCU_TRAFFIC.get("mode_product_tc2_p3" if cs else "mode_product_tc2_sym")
                 if (args.precision == "bf16x3" and n == 768) else None,
                 "traffic_unit": "bytes/launch (ncu, DRAM read+write)",
-                "kernel": (f"mode_product_tc2_kernel ({args.precision}, 2-CTA tcgen05, MN-major A, symmetric "
-                           "tiles), the third product" if cs else
+                "kernel": (f"mode_product_tc2_kernel ({args.precision}, 2-CTA tcgen05, MN-major A, row tiles "
+                           "a/256 <= b/256, K3 stored by its full symmetry), the third product" if cs else
                            f"mode_product_tc2_kernel ({args.precision}, 2-CTA tcgen05, symmetric tiles), "
                            "2 launches/step (P2, P3)"),
                 "flops_per_launch": flops_launch, "avg_launch_ms": round(mp_ms, 4),
@@ -665,8 +683,9 @@ def main():
             p2_ms = float(phases[4])
             a2 = p2_flops / (p2_ms * 1e-3) / 1e12
             roof["second_product"] = {
-                "kernel": "mode_product_tc2_kernel, grouped by atom (K = Kc), symmetric in (p, q) with transposed "
-                          "stores", "Mp": Mp, "Kc": Kc, "flops_per_launch": p2_flops, "ms": round(p2_ms, 4),
+                "kernel": "mode_product_tc2_kernel, grouped by atom (K = Kc), tiles p/256 <= q/256 of U2 only "
+                          "(symmetric in (p, q))", "Mp": Mp, "Kc": Kc, "flops_per_launch": p2_flops,
+                "ms": round(p2_ms, 4),
                 "achieved": round(a2, 2), "frac": round(a2 / pk, 4) if pk else None,
                 "traffic": NCU_TRAFFIC.get("mode_product_tc2_p2") if (args.precision == "bf16x3" and n == 768)
                 else None}
@@ -729,6 +748,19 @@ def main():
         f1.record(stream)
         torch.cuda.synchronize()
         fp32_info["dense_products_s_per_snapshot"] = f0.elapsed_time(f1) / nf / 1e3
+        if cs:   # the same step with the opt-in packed K3 (device-resident)
+            kpk = julia_tensor((fcb.packed_k3_count(n),), np.float32, dev)
+            kp = prec | _lib.FCB_K3_PACKED
+            step(precision=kp, k3_ptr=int(kpk.data_ptr()))
+            pph = profile_phases(kp, reps=1)
+            pk_fl = full_sym_executed_flops(cs[0], n, n, packed=True)
+            packed_info = {"s_per_snapshot": timed(lambda: step(precision=kp, k3_ptr=int(kpk.data_ptr())), stream, nf),
+                           "k3_floats": fcb.packed_k3_count(n), "third_product_ms": round(float(pph[5]), 4),
+                           "third_product_flops": pk_fl,
+                           "third_product_achieved_tflops": round(pk_fl / (float(pph[5]) * 1e-3) / 1e12, 2),
+                           "note": "FCB_K3_PACKED: the third product stores only K3[p,q,s], p <= q <= s, and skips "
+                                   "the mode tiles that hold none"}
+            del kpk
         fp32_info["speedup_split_vs_fp32_both_dense"] = fp32_s / fp32_info["dense_products_s_per_snapshot"]
         if args.precision == "bf16x3" and not args.skip_extra:
             # TF32x3 on the same step: time, error and its third product against the measured TF32 GEMM
@@ -780,6 +812,22 @@ def main():
         e2e["with_psi64_to_host"] = {"value": (time.perf_counter() - t0) / ne, "unit": UNIT,
                                      "d2h_bytes_per_step": int(k3_h.numel() * 4 + psi_h.numel() * 8)}
         del psi_h
+        # opt-in packed K3 (FCB_K3_PACKED): only the entries p <= q <= s come back
+        if split:
+            kp = prec | _lib.FCB_K3_PACKED
+            kp_h = torch.empty(fcb.packed_k3_count(n), dtype=torch.float32).pin_memory()
+            step(precision=kp, k3_ptr=int(kp_h.data_ptr()), phi_ptr=int(phi_h.data_ptr()), pos_ptr=pos_h.ctypes.data)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(ne):
+                step(precision=kp, k3_ptr=int(kp_h.data_ptr()), phi_ptr=int(phi_h.data_ptr()),
+                     pos_ptr=pos_h.ctypes.data)
+            torch.cuda.synchronize()
+            e2e["packed_k3"] = {"value": (time.perf_counter() - t0) / ne, "unit": UNIT,
+                                "h2d_bytes_per_step": int(pos_h.nbytes + phi_h.numel() * 4),
+                                "d2h_bytes_per_step": int(kp_h.numel() * 4),
+                                "note": "FCB_K3_PACKED: the M(M+1)(M+2)/6 entries p <= q <= s of the symmetric K3"}
+            del kp_h
 
     batch = None
     if not args.skip_batch:

@@ -275,7 +275,7 @@ int fcb200_trim(fcb200_handle h) {
     Buf* bufs[] = {&h->pos, &h->box, &h->masses, &h->pair_t, &h->pair_flag, &h->self_t, &h->psi_stage,
                    &h->phi_f32, &h->phi_hi, &h->phi_lo, &h->psi_hi, &h->psi_lo, &h->u1_hi, &h->u1_lo,
                    &h->u2_hi, &h->u2_lo, &h->u1_f32, &h->u2_f32, &h->psi_f32, &h->k3_stage[0],
-                   &h->k3_stage[1], &h->ifc2, &h->sw_ints, &h->sw_nbr_r, &h->sw_pair_off, &h->sw_blk3,
+                   &h->k3_stage[1], &h->k3_full, &h->ifc2, &h->sw_ints, &h->sw_nbr_r, &h->sw_pair_off, &h->sw_blk3,
                    &h->sw_blk2, &h->sw_atoms, &h->sw_place, &h->sw_col_off, &h->sw_col_items, &h->sw_cursor,
                    &h->sw_asr_off, &h->sw_asr_items, &h->sw_asr, &h->adj_phiT, &h->adj_w_hi, &h->adj_w_lo,
                    &h->adj_pairs, &h->adj_G, &h->adj_scal, &h->adj_w32, &h->adj_dpos, &h->adj_w64,
@@ -584,7 +584,8 @@ namespace {
 // three mode products run.
 template <class Assemble>
 int snapshot_run(fcb200_context* h, int64_t N, const float* phi, int64_t mode_lo, int64_t mode_hi, int precision,
-                 double* psi_out, float* k3_out, cudaStream_t s, bool host_inputs, Assemble assemble) {
+                 double* psi_out, float* k3_out, cudaStream_t s, bool host_inputs, Assemble assemble,
+                 bool packed = false) {
     const int64_t n = 3 * N;
     float* d_phi;
     FCB_TRY(device_view(h->phi_f32, phi, (size_t)(n * n), true, s, &d_phi));
@@ -615,17 +616,24 @@ int snapshot_run(fcb200_context* h, int64_t N, const float* phi, int64_t mode_lo
     phase_mark(h, s, 2);
     if (precision == FCB_MCC3_FP32) phase_mark(h, s, 3);  // no φ split phase
     const int64_t M = mode_hi - mode_lo;
+    const int64_t k3n = packed ? packed_k3_count(M) : M * M * M;
     float* d_k3;
-    FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)(M * M * M), false, s, &d_k3));
-    FCB_TRY(run_mcc3(h, precision, op, d_phi, n, mode_lo, mode_hi, mode_lo, mode_hi, mode_lo, mode_hi, d_k3, s,
+    FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)k3n, false, s, &d_k3));
+    float* d_full = d_k3;
+    if (packed) {  // the full K3 into scratch, then its unique entries
+        FCB_TRY(h->k3_full.ensure(sizeof(float) * (size_t)(M * M * M)));
+        d_full = h->k3_full.as<float>();
+    }
+    FCB_TRY(run_mcc3(h, precision, op, d_phi, n, mode_lo, mode_hi, mode_lo, mode_hi, mode_lo, mode_hi, d_full, s,
                      true));
+    if (packed) FCB_TRY(pack_k3_launch(d_full, M, d_k3, s));
     bool host = host_inputs || d_phi != phi;
     if (host64) {
         FCB_CUDA(cudaMemcpyAsync(psi_out, out.psi64, sizeof(double) * n * n * n, cudaMemcpyDeviceToHost, s));
         host = true;
     }
     if (d_k3 != k3_out) {
-        FCB_CUDA(cudaMemcpyAsync(k3_out, d_k3, sizeof(float) * M * M * M, cudaMemcpyDeviceToHost, s));
+        FCB_CUDA(cudaMemcpyAsync(k3_out, d_k3, sizeof(float) * k3n, cudaMemcpyDeviceToHost, s));
         host = true;
     }
     if (host) return check_status(h, s);
@@ -689,7 +697,7 @@ int sparse_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, in
 template <class Hook>
 int compact_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, int kind, int cap, const int* d_nb,
                      const int* d_count, const int* d_self, double tol, const double* d_m, const float* d_phi,
-                     float* d_k3, cudaStream_t s, Hook hook) {
+                     float* d_k3, cudaStream_t s, Hook hook, bool packed = false) {
     const int64_t n = 3 * N;
     const int64_t np = pad_for(kind, n);
     const int64_t Mp = compact_Mp(M), Kc = compact_Kc(cap);
@@ -708,6 +716,7 @@ int compact_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, i
     FCB_TRY(h->u2_lo.ensure(esz * Mp * n * M));
     ModeProduct p2{Mp * n, Kc, M, Kc, Kc, Mp, Mp, Mp * n};
     p2.sym_inner = true;
+    p2.inner_upper = true;  // U2 tiles with p / 256 <= q / 256 only: all the third product reads
     p2.b_group = 3 * Mp;
     p2.b_group_ld = M;
     FCB_TRY(mode_product_tc(h, kind, h->u1_hi.p, h->u1_lo.p, h->phik_hi.p, h->phik_lo.p, h->u2_hi.p, h->u2_lo.p, kind,
@@ -716,7 +725,8 @@ int compact_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, i
     FCB_TRY(hook());
     const size_t poff = esz * np * mode_lo;
     ModeProduct p3{Mp * M, n, M, Mp, np, Mp, M, M * M};
-    p3.sym = true;
+    p3.sym_full = true;  // row tiles with p / 256 <= q / 256, K3 stored by its full symmetry
+    p3.packed = packed;  // or only its unique entries, packed
     p3.a_mn = true;
     p3.lda_z = Mp * n;
     p3.Fv = M;
@@ -726,13 +736,21 @@ int compact_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, i
 
 // The compact form where it applies, else the dense-layout sparse form; the
 // hook runs once, before the third product or after the first.
+// With `packed`, d_k3 receives the unique entries only: written directly by
+// the compact third product, else packed from a full K3 in scratch.
 template <class Hook>
 int sparse_snapshot_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, int kind, int cap,
                              const int* d_nb, const int* d_count, const int* d_self, double tol, const double* d_m,
-                             const float* d_phi, float* d_k3, cudaStream_t s, Hook hook) {
+                             const float* d_phi, float* d_k3, cudaStream_t s, Hook hook, bool packed = false) {
     if (tc_pair_enabled() && compact_pays(3 * N, M, cap))
-        return compact_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s, hook);
-    return sparse_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s, hook);
+        return compact_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s, hook,
+                                packed);
+    if (!packed)
+        return sparse_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s, hook);
+    FCB_TRY(h->k3_full.ensure(sizeof(float) * (size_t)(M * M * M)));
+    FCB_TRY(sparse_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi,
+                            h->k3_full.as<float>(), s, hook));
+    return pack_k3_launch(h->k3_full.as<float>(), M, d_k3, s);
 }
 
 // The LJ snapshot with a block-sparse first mode product (split precisions).
@@ -749,7 +767,7 @@ int sparse_snapshot_products(fcb200_context* h, int64_t N, int64_t mode_lo, int6
 int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const double* d_box, double sigma,
                        double eps, double r_cut, double tol, const double* d_m, const float* phi, int64_t mode_lo,
                        int64_t mode_hi, int precision, double* psi_out, float* k3_out, cudaStream_t s,
-                       bool host_inputs, bool* used) {
+                       bool host_inputs, bool* used, bool packed) {
     *used = false;
     const int64_t n = 3 * N, M = mode_hi - mode_lo;
     const int kind = precision == FCB_MCC3_BF16X3 ? 1 : 2;
@@ -791,8 +809,9 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
     if (cap < 1 || sparse_p1_smem_bytes(cap, N) > 200 * 1024) return FCB_OK;
     *used = true;
     phase_mark(h, s, 2);
+    const int64_t k3n = packed ? packed_k3_count(M) : M * M * M;
     float* d_k3;
-    FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)(M * M * M), false, s, &d_k3));
+    FCB_TRY(device_view(h->k3_stage[0], (const float*)k3_out, (size_t)k3n, false, s, &d_k3));
     bool writer = false;
     auto launch_writer = [&]() -> int {
         if (!psi_out || serial_writer) return FCB_OK;
@@ -806,7 +825,7 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
         return FCB_OK;
     };
     const int rc = sparse_snapshot_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi,
-                                            d_k3, s, launch_writer);
+                                            d_k3, s, launch_writer, packed);
     if (writer) FCB_CUDA(cudaStreamWaitEvent(s, h->ev[3], 0));
     FCB_TRY(rc);
     phase_mark(h, s, 6);
@@ -816,7 +835,7 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
         host = true;
     }
     if (d_k3 != k3_out) {
-        FCB_CUDA(cudaMemcpyAsync(k3_out, d_k3, sizeof(float) * M * M * M, cudaMemcpyDeviceToHost, s));
+        FCB_CUDA(cudaMemcpyAsync(k3_out, d_k3, sizeof(float) * k3n, cudaMemcpyDeviceToHost, s));
         host = true;
     }
     if (host) return check_status(h, s);
@@ -871,7 +890,8 @@ int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t N, const doub
     const int64_t n = 3 * N;
     if (!mcc3_ranges_ok(n, mode_lo, mode_hi)) return set_error(FCB_ERR_ARG, "mode window outside [0, n)");
     const bool force_dense = (precision & FCB_MCC3_FORCE_DENSE) != 0;
-    precision &= ~FCB_MCC3_FORCE_DENSE;
+    const bool packed = (precision & FCB_K3_PACKED) != 0;
+    precision &= ~(FCB_MCC3_FORCE_DENSE | FCB_K3_PACKED);
     FCB_TRY(check_precision(precision));
     double bh[3];
     FCB_TRY(box_to_host(box, bh));
@@ -887,15 +907,17 @@ int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t N, const doub
     if (precision != FCB_MCC3_FP32 && !force_dense) {
         bool used = false;
         FCB_TRY(snapshot_lj_sparse(h, d_pos, N, d_box, sigma, eps, r_cut, tol, d_m, phi, mode_lo, mode_hi, precision,
-                                   psi_out, k3_out, s, d_pos != pos, &used));
+                                   psi_out, k3_out, s, d_pos != pos, &used, packed));
         if (used) return FCB_OK;
     }
-    return snapshot_run(h, N, phi, mode_lo, mode_hi, precision, psi_out, k3_out, s, d_pos != pos,
-                        [&](const AssemblyOut& out) {
-                            FCB_TRY(lj_pair_tables(h, d_pos, N, d_box, sigma, eps, r_cut, s));
-                            phase_mark(h, s, 1);
-                            return ifc3_dense_write(h, N, tol, d_m, out, s);
-                        });
+    return snapshot_run(
+        h, N, phi, mode_lo, mode_hi, precision, psi_out, k3_out, s, d_pos != pos,
+        [&](const AssemblyOut& out) {
+            FCB_TRY(lj_pair_tables(h, d_pos, N, d_box, sigma, eps, r_cut, s));
+            phase_mark(h, s, 1);
+            return ifc3_dense_write(h, N, tol, d_m, out, s);
+        },
+        packed);
 }
 
 int fcb200_mcc3_adjoint_lj(fcb200_handle h, const double* pos, int64_t N, const double* box, double sigma,
@@ -948,6 +970,8 @@ int fcb200_snapshot_sw(fcb200_handle h, const double* pos, int64_t N, const doub
     if (!phi || !k3_out) return set_error(FCB_ERR_ARG, "phi and k3_out must not be NULL");
     const int64_t n = 3 * N;
     if (!mcc3_ranges_ok(n, mode_lo, mode_hi)) return set_error(FCB_ERR_ARG, "mode window outside [0, n)");
+    const bool packed = (precision & FCB_K3_PACKED) != 0;
+    precision &= ~FCB_K3_PACKED;
     FCB_TRY(check_precision(precision));
     cudaSetDevice(h->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -955,11 +979,13 @@ int fcb200_snapshot_sw(fcb200_handle h, const double* pos, int64_t N, const doub
     FCB_TRY(device_view(h->pos, pos, 3 * N, true, s, &d_pos));
     FCB_TRY(device_view(h->box, box, 3, true, s, &d_box));
     FCB_TRY(device_view(h->masses, masses, N, true, s, &d_m));
-    return snapshot_run(h, N, phi, mode_lo, mode_hi, precision, psi_out, k3_out, s, d_pos != pos,
-                        [&](const AssemblyOut& out) {
-                            phase_mark(h, s, 1);
-                            return sw_third_order_launch(h, d_pos, N, d_box, r_cut, cos0, tol, d_m, out, s);
-                        });
+    return snapshot_run(
+        h, N, phi, mode_lo, mode_hi, precision, psi_out, k3_out, s, d_pos != pos,
+        [&](const AssemblyOut& out) {
+            phase_mark(h, s, 1);
+            return sw_third_order_launch(h, d_pos, N, d_box, r_cut, cos0, tol, d_m, out, s);
+        },
+        packed);
 }
 
 // ---------------------------------------------------------------------------

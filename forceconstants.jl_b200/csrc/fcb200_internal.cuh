@@ -77,6 +77,7 @@ struct fcb200_context {
     fcb::Buf u1_f32, u2_f32;        // plain FP32 intermediates
     fcb::Buf psi_f32;               // staged Ψ (FP32) for host inputs
     fcb::Buf k3_stage[2];           // K3 staging slabs (device) for host outputs
+    fcb::Buf k3_full;               // full K3 before packing (FCB_K3_PACKED on the dense paths)
     fcb::Buf ifc2;                  // second-order scratch
     // Stillinger-Weber scratch (neighbours, blocks, placements, buckets, ASR rows)
     fcb::Buf sw_ints, sw_nbr_r, sw_pair_off, sw_blk3, sw_blk2, sw_atoms, sw_place;
@@ -202,6 +203,22 @@ struct ModeProduct {
     // tiles wholly below the diagonal are skipped and tiles wholly above it are
     // also stored transposed.  F a multiple of 256; mode tiles 256 wide.
     bool sym_inner = false;
+    // With sym_inner: store the computed tiles only (no transposed copies); the
+    // tiles below the (p, q) tile diagonal stay unwritten, for a consumer that
+    // reads only tiles with p / 256 <= q / 256 (sym_full).
+    bool inner_upper = false;
+    // Output symmetric in all three indices (K3 of an assembled IFC3 over equal
+    // mode windows): rows r = a + F·b (rows with a >= Fv are padding), columns
+    // s, T(x) = x / 256.  Only row tiles with T(a) <= T(b) are computed (every
+    // column), and each computed entry is stored at (a,b,s), at (a,s,b) when
+    // T(s) < T(a), at (s,a,b) when T(s) > T(b) and at (s,b,a) when
+    // T(s) > T(b) > T(a): every entry of the output exactly once.  FP32 output,
+    // F a multiple of 256, R = F·M, 256-wide mode tiles.
+    bool sym_full = false;
+    // With sym_full: store only the entries a <= b <= s, each once, into the
+    // packed layout s(s+1)(s+2)/6 + b(b+1)/2 + a (FCB_K3_PACKED) instead of
+    // the M³ output.
+    bool packed = false;
     // A read MN-major: A[r,a] at (r % F) + lda·a + lda_z·(r / F); F a multiple
     // of 128 and R of F.
     bool a_mn = false;
@@ -215,6 +232,10 @@ struct ModeProduct {
 
 int mode_product_f32(const float* A, const float* B, float* D, const ModeProduct& mp,
                      cudaStream_t s);
+// Packed symmetry-unique copy of a full M³ K3: packed[s(s+1)(s+2)/6 + q(q+1)/2 + p]
+// = K3[p + M(q + M s)] for p <= q <= s (mcc3.cu).
+int pack_k3_launch(const float* full, int64_t M, float* packed, cudaStream_t s);
+inline int64_t packed_k3_count(int64_t M) { return M * (M + 1) * (M + 2) / 6; }
 // FP64 (DFMA) mode product and an FP32 → FP64 widening copy (mode_product_f64.cu).
 int mode_product_f64(const double* A, const double* B, double* D, const ModeProduct& mp, cudaStream_t s);
 int widen_f32_to_f64(const float* src, double* dst, int64_t count, cudaStream_t s);

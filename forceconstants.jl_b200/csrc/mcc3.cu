@@ -40,7 +40,25 @@ __global__ void split_kernel(const float* __restrict__ src, int64_t rows, int64_
     }
 }
 
+// One CTA per (q, s), q <= s: the run K3[0..q, q, s] (contiguous in the full
+// layout) to packed[s(s+1)(s+2)/6 + q(q+1)/2 + p].
+__global__ void pack_k3_kernel(const float* __restrict__ full, int64_t M, float* __restrict__ packed) {
+    const int64_t q = blockIdx.x, s = blockIdx.y;
+    if (q > s) return;
+    const int64_t base = s * (s + 1) * (s + 2) / 6 + q * (q + 1) / 2;
+    const float* src = full + M * (q + M * s);
+    for (int64_t p = threadIdx.x; p <= q; p += blockDim.x) packed[base + p] = src[p];
+}
+
 }  // namespace
+
+int pack_k3_launch(const float* full, int64_t M, float* packed, cudaStream_t s) {
+    if (M <= 0) return FCB_OK;
+    if (M > 65535) return set_error(FCB_ERR_ARG, "packed K3: too many modes");
+    pack_k3_kernel<<<dim3((unsigned)M, (unsigned)M), 128, 0, s>>>(full, M, packed);
+    FCB_CUDA(cudaGetLastError());
+    return FCB_OK;
+}
 
 int split_operand(const float* src, int64_t rows, int64_t cols, int64_t ld_src, void* hi, void* lo,
                   int64_t ld_dst, int kind, cudaStream_t s) {

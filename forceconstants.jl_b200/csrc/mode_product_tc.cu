@@ -57,7 +57,10 @@ struct TcParams {
     int64_t F, F_pad, ldd;
     int bn, n_tiles, m_tiles, k_chunks, elems_per_row;
     int out_kind;
-    int sym;  // symmetric output (pair kernel): 1 = ModeProduct::sym, 2 = ModeProduct::sym_inner
+    int sym;  // symmetric output (pair kernel): 1 = ModeProduct::sym, 2 = ModeProduct::sym_inner,
+              // 3 = ModeProduct::sym_full
+    int inner_upper;               // ModeProduct::inner_upper (with sym 2)
+    int packed;                    // ModeProduct::packed (with sym 3)
     int vec;  // F, F_pad, ldd multiples of 8: 8 consecutive rows are 8 consecutive, aligned elements
     int a_mn;                      // A read MN-major through a 3-D map (ModeProduct::a_mn)
     int64_t b_group, b_group_ld;   // ModeProduct::b_group / b_group_ld (pair kernel)
@@ -310,8 +313,19 @@ __device__ __forceinline__ void store_vec8(const TcParams& p, int64_t off, const
 
 // Symmetric output: does pair tile (mt, nt) hold any column >= its rows' outer
 // index (sym 1), or any column >= its rows' inner index (sym 2: the 256 rows of
-// a tile share one outer index and the tiles are square)?
+// a tile share one outer index and the tiles are square)?  With full symmetry
+// (sym 3) a row tile is computed, every column of it, when T(a) <= T(b); with
+// the packed output only its mode tiles that reach s >= b.
 __device__ __forceinline__ bool sym_tile_live(const TcParams& p, int mt, int nt) {
+    if (p.sym == 3) {
+        const int64_t r0 = (int64_t)mt * 256, a0 = r0 % p.F, b = r0 / p.F;
+        if (p.packed) {  // only entries a <= b <= s are stored
+            int64_t smax = (int64_t)nt * p.bn + p.bn;
+            if (smax > p.M) smax = p.M;
+            return a0 <= b && smax - 1 >= b;
+        }
+        return a0 / 256 <= b / 256;
+    }
     const int64_t pmin = p.sym == 2 ? ((int64_t)mt * 256) % p.F : ((int64_t)mt * 256) / p.F;
     int64_t qmax = (int64_t)nt * p.bn + p.bn;
     if (qmax > p.M) qmax = p.M;
@@ -878,7 +892,8 @@ __global__ void __maxnreg__(128)
             const int64_t wrow0 = (int64_t)mt * 256 + rank * 128 + q * 32;  // the warp's first row
             const bool warp_vec = p.vec && wrow0 + 32 <= p.R;
             // sym 2: a tile wholly above the diagonal is also stored transposed
-            const bool sym2_mirror = p.sym == 2 && (int64_t)nt * p.bn >= ((int64_t)mt * 256) % p.F + 256;
+            const bool sym2_mirror =
+                p.sym == 2 && !p.inner_upper && (int64_t)nt * p.bn >= ((int64_t)mt * 256) % p.F + 256;
             float* stg = stage_base + (warp - 2) * (32 * STG_LD);
             for (int ch = cpar; ch < chunks; ch += EPI / 4) {
                 uint32_t v[32];
@@ -920,6 +935,62 @@ __global__ void __maxnreg__(128)
                         __syncwarp();
                         continue;
                     }
+                }
+                if (p.sym == 3) {
+                    // Full symmetry: the warp's 32 rows a0.. share b, the chunk's
+                    // columns share T(s); which images to store is decided per
+                    // block (the host guarantees FP32 TMA output and 8-aligned
+                    // shapes, and the boxes are clipped at M by the map).
+                    const int64_t b = wrow0 / p.F, a0 = wrow0 - b * p.F;
+                    if (ncols <= 0 || a0 >= p.Fv) continue;  // no columns, or padding rows only
+                    if (p.packed) {
+                        // only a <= b <= s, each entry once: for column s the run a = 0..b
+                        // sits at s(s+1)(s+2)/6 + b(b+1)/2, so a warp's store of one column
+                        // is 32 consecutive floats (fewer where the run ends at b)
+                        if (a0 > b || c0 + ncols <= b) continue;
+                        const int64_t a = a0 + lane;
+                        float* dst = static_cast<float*>(p.d_hi) + b * (b + 1) / 2 + a;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int64_t sc = c0 + j;
+                            if (j < ncols && sc >= b && a <= b) dst[sc * (sc + 1) * (sc + 2) / 6] = __uint_as_float(v[j]);
+                        }
+                        continue;
+                    }
+                    const int64_t ta = a0 >> 8, tb = b >> 8, ts = c0 >> 8;
+                    // [s][a] lines: the direct box (a, b, s) and, when T(s) < T(a), the mirrored (a, s, b)
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        stg[j * 32 + ((((lane >> 2) ^ j) & 7) << 2) + (lane & 3)] = __uint_as_float(v[j]);
+                    fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0) {
+                        tma_store_3d(&mD, stg, (int)a0, (int)b, (int)c0);
+                        if (ts < ta) tma_store_3d(&mDt, stg, (int)a0, (int)c0, (int)b);
+                        bulk_commit();
+                    }
+                    __syncwarp();
+                    if (ts > tb) {
+                        // [a][s] lines (each lane its own row, 16-byte chunks swizzled by
+                        // line): the transposed images (s, a, b) and, when T(b) > T(a), (s, b, a)
+                        if (lane == 0) bulk_wait_read();
+                        __syncwarp();
+                        float* line = stg + lane * 32;
+#pragma unroll
+                        for (int g = 0; g < 8; ++g)
+                            *reinterpret_cast<float4*>(line + ((g ^ (lane & 7)) << 2)) =
+                                make_float4(__uint_as_float(v[4 * g]), __uint_as_float(v[4 * g + 1]),
+                                            __uint_as_float(v[4 * g + 2]), __uint_as_float(v[4 * g + 3]));
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) {
+                            tma_store_3d(&mDt, stg, (int)c0, (int)a0, (int)b);
+                            if (tb > ta) tma_store_3d(&mD, stg, (int)c0, (int)b, (int)a0);
+                            bulk_commit();
+                        }
+                        __syncwarp();
+                    }
+                    continue;
                 }
                 if (p.tma_out == 1 && warp_vec && ncols > 0 && (ncols == 32 || c0 + ncols == p.M)) {
                     // FP32 output by TMA: the warp's 32 rows share one outer index
@@ -1205,7 +1276,10 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
     p.F = mp.F;
     p.F_pad = mp.F_pad;
     p.ldd = mp.ldd;
-    p.sym = mp.sym_inner ? 2 : mp.sym ? 1 : 0;
+    p.sym = mp.sym_full ? 3 : mp.sym_inner ? 2 : mp.sym ? 1 : 0;
+    p.inner_upper = mp.inner_upper ? 1 : 0;
+    p.packed = mp.packed ? 1 : 0;
+    if (mp.packed && !mp.sym_full) return set_error(FCB_ERR_ARG, "mode_product_tc: packed output needs full symmetry");
     p.vec = (mp.F % 8 == 0 && mp.F_pad % 8 == 0 && mp.ldd % 8 == 0) ? 1 : 0;
     p.a_mn = mp.a_mn ? 1 : 0;
     p.b_group = mp.b_group;
@@ -1213,7 +1287,7 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
     p.Fv = mp.Fv > 0 ? mp.Fv : mp.F;
     p.tma_out = 0;
     if (mp.sym && mp.R != mp.F * mp.M) return set_error(FCB_ERR_ARG, "mode_product_tc: symmetric output needs R = F*M");
-    const bool ext = mp.sym_inner || mp.a_mn || mp.b_group || p.Fv != mp.F;
+    const bool ext = mp.sym_inner || mp.sym_full || mp.a_mn || mp.b_group || p.Fv != mp.F;
     if (ext) {
         // forms of the 2-CTA kernel only; every warp takes the 16-byte store path
         if (!(use_pair_kernel() && h->sm_count >= 2))
@@ -1222,19 +1296,21 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
             return set_error(FCB_ERR_ARG, "mode_product_tc: grouped / MN-major forms need 8-aligned shapes");
         if (mp.sym_inner && (mp.sym || mp.F % 256 != 0 || out_kind != kind))
             return set_error(FCB_ERR_ARG, "mode_product_tc: inner symmetry needs 256-row blocks");
+        if (mp.sym_full && (mp.sym || mp.sym_inner || out_kind != 0 || mp.F % 256 != 0 || mp.R != mp.F * mp.M))
+            return set_error(FCB_ERR_ARG, "mode_product_tc: full symmetry needs FP32 output, 256-row blocks, R = F*M");
         if (mp.a_mn && (mp.F % 128 != 0 || mp.R % mp.F != 0))
             return set_error(FCB_ERR_ARG, "mode_product_tc: MN-major A needs 128-row blocks");
         if (mp.b_group && mp.b_group % 256 != 0)
             return set_error(FCB_ERR_ARG, "mode_product_tc: B groups must hold whole 256-row tiles");
     }
     p.n_tiles = (int)((mp.M + BN_MAX - 1) / BN_MAX);
-    if (h->tune && !mp.sym_inner) {  // autotuned mode-tile count for this shape, if any
+    if (h->tune && !mp.sym_inner && !mp.sym_full) {  // autotuned mode-tile count for this shape, if any
         auto it = h->tune->find(tune_key(kind, mp.R, mp.K, mp.M));
         if (it != h->tune->end() && it->second >= p.n_tiles && it->second <= mp.M) p.n_tiles = it->second;
     }
     const int64_t per = (mp.M + p.n_tiles - 1) / p.n_tiles;
     p.bn = (int)(((per + 15) / 16) * 16);
-    if (mp.sym_inner && mp.M > 256) p.bn = 256;  // square 256 × 256 tiles
+    if ((mp.sym_inner || mp.sym_full) && mp.M > 256) p.bn = 256;  // square 256 × 256 tiles
     p.m_tiles = (int)((mp.R + BM - 1) / BM);
     p.elems_per_row = ROW_BYTES / (kind == 1 ? 2 : 4);
     p.k_chunks = (int)((mp.K + p.elems_per_row - 1) / p.elems_per_row);
@@ -1267,14 +1343,22 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
         // direct and mirrored, when a warp's 32 rows share one outer index
         CUtensorMap md = ma_hi, mdt = ma_hi;
         p.tma_out = 0;
-        if (out_kind == 0 && mp.sym && p.vec && mp.F % 32 == 0 && mp.R == mp.F * mp.M) {
+        if (out_kind == 0 && (mp.sym || mp.sym_full) && p.vec && mp.F % 32 == 0 && mp.R == mp.F * mp.M) {
             FCB_TRY(make_map_out(&md, D_hi, p.Fv, mp.M, mp.M, mp.F_pad, mp.ldd, false));
             FCB_TRY(make_map_out(&mdt, D_hi, p.Fv, mp.M, mp.M, mp.F_pad, mp.ldd, true));
             p.tma_out = 1;
         }
+        if (mp.sym_full && p.tma_out != 1)
+            return set_error(FCB_ERR_ARG, "mode_product_tc: full symmetry needs the TMA-stored FP32 output");
         // BF16 planes with inner symmetry (the grouped second product): one map
         // per plane, (row in block, block, column), serves the direct box and,
-        // with the roles of row and column exchanged, the transposed one
+        // with the roles of row and column exchanged, the transposed one.  Its
+        // first dimension is F (= Mp), not M: rows p in [M, Mp) are stored too,
+        // as the zeros their zero U1c rows give, so that the third product,
+        // which reads those padding rows as A rows (and stores none of the K3
+        // rows they produce, Fv = M), never reads unwritten memory.  The
+        // transposed box, where used, may carry accumulator columns past M
+        // (B rows of the next group); they land in padding rows p >= M only.
         if (kind == 1 && out_kind == 1 && mp.sym_inner && p.vec) {
             FCB_TRY(make_map_out(&md, D_hi, mp.F, mp.R / mp.F, mp.M, mp.F_pad, mp.ldd, false, true));
             FCB_TRY(make_map_out(&mdt, D_lo, mp.F, mp.R / mp.F, mp.M, mp.F_pad, mp.ldd, false, true));

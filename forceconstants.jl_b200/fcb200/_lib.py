@@ -26,6 +26,7 @@ FCB_MCC3_BF16X3 = 1
 FCB_MCC3_TF32X3 = 2
 FCB_ADJOINT_FP64 = 3
 FCB_MCC3_FORCE_DENSE = 0x100
+FCB_K3_PACKED = 0x200
 PRECISIONS = {"fp32": FCB_MCC3_FP32, "bf16x3": FCB_MCC3_BF16X3, "tf32x3": FCB_MCC3_TF32X3}
 # The adjoint also forms G in FP64 (FCB_ADJOINT_FP64).
 ADJOINT_PRECISIONS = dict(PRECISIONS, fp64=FCB_ADJOINT_FP64)

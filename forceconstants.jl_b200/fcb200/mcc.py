@@ -75,29 +75,60 @@ def mcc3_window(psi, phi, n_range, m_range, l_range, precision: str = "fp32"):
 
 
 def snapshot_lj(sys, pot, calc, phi, precision: str = "bf16x3", modes=None, psi_out=None, k3_out=None,
-                stream: int = 0, dense: bool = False):
+                stream: int = 0, dense: bool = False, packed: bool = False):
     """Fused third_order → mass_weight_third_order! → Float32 → mcc3 for one
     snapshot (LJ, or Stillinger-Weber when ``pot`` is a
     StillingerWeberSilicon), without the host round trip.  Buffers may be host
     or device; returns (psi_out, k3_out).  For LJ with a split precision the
-    first two mode products use the block sparsity of Ψ unless ``dense``."""
+    first two mode products use the block sparsity of Ψ unless ``dense``.
+    With ``packed`` the K3 output holds only the entries p <= q <= s
+    (``unpack_k3`` restores the full tensor)."""
     from .types import StillingerWeberSilicon
     n = 3 * sys.n_atoms
     lo, hi = (0, n) if modes is None else (int(modes[0]), int(modes[1]))
     M = hi - lo
     if k3_out is None:
-        k3_out = julia_empty((M, M, M), np.float32, "cuda" if is_torch(phi) and phi.is_cuda else "cpu")
+        where = "cuda" if is_torch(phi) and phi.is_cuda else "cpu"
+        k3_out = julia_empty((packed_k3_count(M),) if packed else (M, M, M), np.float32, where)
     dev = device_index(phi) if is_torch(phi) else 0
+    flags = _lib.FCB_K3_PACKED if packed else 0
     if isinstance(pot, StillingerWeberSilicon):
         c0 = np.array([-0.333333333333, float(pot.cos0)], dtype=np.float64)
         _lib.check(_lib.lib().fcb200_snapshot_sw(
             _lib.handle(dev), ptr(sys.positions), sys.n_atoms, ptr(sys.box_sizes), float(calc.r_cut),
-            float(calc.tol), ptr(c0), ptr(sys.masses), ptr(phi), lo, hi, _lib.PRECISIONS[precision],
+            float(calc.tol), ptr(c0), ptr(sys.masses), ptr(phi), lo, hi, _lib.PRECISIONS[precision] | flags,
             ptr(psi_out), ptr(k3_out), stream or stream_ptr(k3_out)))
         return psi_out, k3_out
     _lib.check(_lib.lib().fcb200_snapshot_lj(
         _lib.handle(dev), ptr(sys.positions), sys.n_atoms, ptr(sys.box_sizes), float(pot.sigma), float(pot.eps),
         float(calc.r_cut), float(calc.tol), ptr(sys.masses), ptr(phi), lo, hi,
-        _lib.PRECISIONS[precision] | (_lib.FCB_MCC3_FORCE_DENSE if dense else 0),
+        _lib.PRECISIONS[precision] | (_lib.FCB_MCC3_FORCE_DENSE if dense else 0) | flags,
         ptr(psi_out), ptr(k3_out), stream or stream_ptr(k3_out)))
     return psi_out, k3_out
+
+
+def packed_k3_count(M: int) -> int:
+    """Entries K3[p,q,s] with p <= q <= s of an M-mode K3 (FCB_K3_PACKED)."""
+    return M * (M + 1) * (M + 2) // 6
+
+
+def packed_k3_index(M: int):
+    """Flat column-major index p + M(q + M s) of the full K3 for every packed
+    position (entry (p,q,s), p <= q <= s, at s(s+1)(s+2)/6 + q(q+1)/2 + p)."""
+    s = np.repeat(np.arange(M), [(x + 1) * (x + 2) // 2 for x in range(M)])
+    q = np.concatenate([np.repeat(np.arange(x + 1), np.arange(1, x + 2)) for x in range(M)])
+    base = s * (s + 1) * (s + 2) // 6 + q * (q + 1) // 2
+    p = np.arange(packed_k3_count(M)) - base
+    return p + M * (q + M * s)
+
+
+def unpack_k3(packed, M: int) -> np.ndarray:
+    """The full symmetric K3 (M×M×M, column-major) from its packed entries."""
+    vals = np.asarray(packed.cpu() if is_torch(packed) else packed, dtype=np.float32).reshape(-1)
+    idx = packed_k3_index(M)
+    p, rest = idx % M, idx // M
+    q, s = rest % M, rest // M
+    out = np.empty((M, M, M), dtype=np.float32, order="F")
+    for a, b, c in ((p, q, s), (p, s, q), (q, p, s), (q, s, p), (s, p, q), (s, q, p)):
+        out[a, b, c] = vals
+    return out

@@ -53,6 +53,13 @@ extern "C" {
 /* OR into the precision of fcb200_snapshot_lj: run the dense first and second
  * mode products even where the block-sparse form applies.                     */
 #define FCB_MCC3_FORCE_DENSE 0x100
+/* OR into the precision of fcb200_snapshot_lj / _sw: k3_out receives only the
+ * symmetry-unique entries K3[p,q,s], p <= q <= s (K3 of an assembled IFC3 is
+ * symmetric in its three indices), p fastest: entry (p,q,s) at
+ * s(s+1)(s+2)/6 + q(q+1)/2 + p, M(M+1)(M+2)/6 floats in all (M modes).  The
+ * reference computes the full tensor and notes the unique part as a TODO
+ * (src/mcc.jl:116-117).                                                        */
+#define FCB_K3_PACKED 0x200
 
 /* ---- flags for fcb200_third_order_* -------------------------------------- */
 #define FCB_PSI_MASS_WEIGHTED 1 /* write Ψ already divided by sqrt(m_i m_j m_k) into psi_out */
@@ -219,7 +226,9 @@ int fcb200_mcc3_blocked(fcb200_handle h, const float* psi, const float* phi, int
  * of 8), P1 written in the dense layout and symmetric dense P2/P3.  Same K3
  * within the mcc3 tolerance; this form synchronises the stream once (after the
  * neighbour lists), and writes psi_out on a second stream beside the last
- * product.  FCB_MCC3_FORCE_DENSE selects the dense products.
+ * product.  FCB_MCC3_FORCE_DENSE selects the dense products; FCB_K3_PACKED
+ * writes only the symmetry-unique entries of K3 (k3_out then holds
+ * M(M+1)(M+2)/6 floats, M = mode_hi - mode_lo).
  */
 int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
                        double sigma, double eps, double r_cut, double tol, const double* masses,
@@ -230,7 +239,8 @@ int fcb200_snapshot_lj(fcb200_handle h, const double* pos, int64_t n_atoms, cons
  * One Stillinger-Weber snapshot end to end: SW IFC3 assembly (as
  * fcb200_third_order_sw) with the fused mass-weighted operand, then mcc3 over
  * modes [mode_lo, mode_hi) on every axis.  Same composition as
- * fcb200_snapshot_lj for the reference's AutoDiffCalculator SW path.
+ * fcb200_snapshot_lj for the reference's AutoDiffCalculator SW path;
+ * FCB_K3_PACKED as there.
  */
 int fcb200_snapshot_sw(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
                        double r_cut, double tol, const double* cos0, const double* masses,

@@ -67,3 +67,46 @@ def test_asr_checker_quirk(fcb):
     assert fcb.asr_satisfied(ifc2, 1, 3, 1e-8)
     ifc2[0, 0] = 1.0
     assert not fcb.asr_satisfied(ifc2, 1, 3, 1e-8)
+
+
+def test_packed_k3_layout_roundtrip(fcb):
+    """The packed K3 layout (entry (p,q,s), p <= q <= s, at
+    s(s+1)(s+2)/6 + q(q+1)/2 + p) and its unpacking on the host."""
+    from fcb200.mcc import packed_k3_index
+    for M in (1, 3, 8, 13):
+        a = np.random.default_rng(M).normal(size=(M, M, M))
+        k = sum(a.transpose(t) for t in ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)))
+        k = np.asfortranarray(k.astype(np.float32))
+        idx = packed_k3_index(M)
+        assert idx.shape[0] == fcb.packed_k3_count(M) == len(set(idx.tolist()))
+        p, q, s = idx % M, (idx // M) % M, idx // (M * M)
+        assert np.all(p <= q) and np.all(q <= s)
+        assert np.array_equal(s * (s + 1) * (s + 2) // 6 + q * (q + 1) // 2 + p, np.arange(idx.shape[0]))
+        assert np.array_equal(fcb.unpack_k3(k.reshape(-1, order="F")[idx], M), k)
+
+
+def test_full_symmetry_store_rules_cover_k3_once():
+    """The third product's full-symmetry schedule: row tiles (a, b) with
+    T(a) <= T(b) (T(x) = x // tile) over every column s, each computed entry
+    stored at (a,b,s), at (a,s,b) when T(s) < T(a), at (s,a,b) when
+    T(s) > T(b), at (s,b,a) when T(s) > T(b) > T(a) — every entry of the
+    M³ output exactly once, for tile widths that divide M or not."""
+    for M, tile in ((11, 4), (12, 4), (9, 3), (7, 8), (13, 5), (10, 256)):
+        t = lambda x: x // tile
+        seen = {}
+        for a in range(M):
+            for b in range(M):
+                if t(a) > t(b):
+                    continue
+                for s in range(M):
+                    ta, tb, ts = t(a), t(b), t(s)
+                    outs = [(a, b, s)]
+                    if ts < ta:
+                        outs.append((a, s, b))
+                    if ts > tb:
+                        outs.append((s, a, b))
+                    if ts > tb > ta:
+                        outs.append((s, b, a))
+                    for o in outs:
+                        seen[o] = seen.get(o, 0) + 1
+        assert len(seen) == M ** 3 and set(seen.values()) == {1}, (M, tile)
