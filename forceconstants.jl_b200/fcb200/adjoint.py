@@ -16,7 +16,7 @@ from . import _lib
 from .arrays import as_julia, device_index, is_torch, ptr, stream_ptr
 
 
-def mcc3_adjoint_lj(sys, pot, calc, phi, W, precision: str = "tf32x3"):
+def mcc3_adjoint_lj(sys, pot, calc, phi, W, precision: str = "fp64"):
     M = int(W.shape[0])
     W = as_julia(W, np.float32)
     phi = as_julia(phi, np.float32)
