@@ -219,6 +219,38 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// 16 TMEM lanes × 4 blocks of 8 FP32 columns in the mma accumulator fragment
+// layout: thread t gets, for block k, v[4k..4k+1] = row t/4, columns
+// 8k + 2(t%4) and +1, and v[4k+2..4k+3] = row t/4 + 8, the same columns.
+__device__ __forceinline__ void tmem_ld_16x256b_x4(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.16x256b.x4.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Four 8×8 BF16 matrices from their mma fragments (register i = matrix i:
+// row t/4, columns 2(t%4) and +1), each written transposed: the shared-memory
+// row given by thread 8i + r receives column r of matrix i (8 rows, 16 bytes).
+__device__ __forceinline__ void stmatrix_x4_trans(uint32_t addr, uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
+    asm volatile("stmatrix.sync.aligned.x4.trans.m8n8.shared.b16 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(r0),
+                 "r"(r1), "r"(r2), "r"(r3)
+                 : "memory");
+}
+
+// hi and lo BF16 planes of two FP32 values (lo = the rounding residual of hi)
+__device__ __forceinline__ void split_bf16x2(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
+    const float x = __uint_as_float(a), y = __uint_as_float(b);
+    const __nv_bfloat162 h = __floats2bfloat162_rn(x, y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(x - __uint_as_float(hi << 16), y - __uint_as_float(hi & 0xFFFF0000u));
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
 __device__ __forceinline__ float tf32_round(float v) {
     uint32_t hb;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(v));
@@ -896,6 +928,55 @@ __global__ void __maxnreg__(128)
                 p.sym == 2 && !p.inner_upper && (int64_t)nt * p.bn >= ((int64_t)mt * 256) % p.F + 256;
             float* stg = stage_base + (warp - 2) * (32 * STG_LD);
             for (int ch = cpar; ch < chunks; ch += EPI / 4) {
+                if constexpr (KIND == 1) {
+                    if (p.tma_out == 2 && warp_vec) {
+                        // BF16 planes by TMA (inner symmetry), staged through stmatrix:
+                        // the accumulator is read in the mma fragment layout (two
+                        // 16-lane halves), packed to hi/lo BF16 pairs, and each 8×8
+                        // block is written transposed into the 64-byte-swizzled
+                        // [column][row] staging of the box, 16 bytes per row.
+                        const int64_t c0 = col0 + ch * 32;
+                        int64_t ncols = p.M - c0;
+                        if (ncols > p.bn - ch * 32) ncols = p.bn - ch * 32;
+                        if (ncols > 32) ncols = 32;
+                        if (ncols > 0 && (ncols == 32 || c0 + ncols == p.M)) {
+                            const int64_t pk = wrow0 / p.F, pp0 = wrow0 - pk * p.F;
+                            uint32_t f0[16], f1[16];
+                            const uint32_t tcol = (uint32_t)(acc * BN_MAX + ch * 32);
+                            tmem_ld_16x256b_x4(tmem_base + ((uint32_t)(q * 32) << 16) + tcol, f0);
+                            tmem_ld_16x256b_x4(tmem_base + ((uint32_t)(q * 32 + 16) << 16) + tcol, f1);
+                            tmem_wait_ld();
+                            if (lane == 0) bulk_wait_read();  // the staging block is free again
+                            __syncwarp();
+                            const uint32_t sbase = saddr(stg);
+                            const int mi = lane >> 3, rr = lane & 7;  // this thread's matrix and row address
+#pragma unroll
+                            for (int g = 0; g < 4; ++g) {
+                                // matrices i = 0..3: rows 8i..8i+7 of the warp, columns 8g..8g+7
+                                uint32_t h0, l0, h1, l1, h2, l2, h3, l3;
+                                split_bf16x2(f0[4 * g], f0[4 * g + 1], h0, l0);
+                                split_bf16x2(f0[4 * g + 2], f0[4 * g + 3], h1, l1);
+                                split_bf16x2(f1[4 * g], f1[4 * g + 1], h2, l2);
+                                split_bf16x2(f1[4 * g + 2], f1[4 * g + 3], h3, l3);
+                                const int j = 8 * g + rr;  // staging line (column)
+                                const uint32_t addr = sbase + (uint32_t)(j * 64 + (((mi ^ (j >> 1)) & 3) << 4));
+                                stmatrix_x4_trans(addr, h0, h1, h2, h3);
+                                stmatrix_x4_trans(addr + 2048, l0, l1, l2, l3);
+                            }
+                            fence_proxy_async_smem();
+                            __syncwarp();
+                            if (lane == 0) {
+                                tma_store_3d(&mD, stg, (int)pp0, (int)pk, (int)c0);
+                                tma_store_3d(&mDt, reinterpret_cast<uint8_t*>(stg) + 2048, (int)pp0, (int)pk, (int)c0);
+                                bulk_commit();
+                            }
+                            __syncwarp();
+                            continue;
+                        }
+                        if (ncols <= 0) continue;
+                        // any other partial chunk takes the general path below
+                    }
+                }
                 uint32_t v[32];
                 tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN_MAX + ch * 32), v);
                 const int64_t c0 = col0 + ch * 32;
