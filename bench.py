@@ -41,13 +41,13 @@ SIGMA, EPS, R_CUT, TOL, MASS = 3.4, 0.24037, 8.5, 1e-12, 39.95
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 # DRAM bytes (read + write) per launch at n = 768, bf16x3, from one 1-pass ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of
-#   python bench.py --steps 2 --warmup 3 --skip-cpu --skip-e2e --skip-batch
+#   python bench.py --steps 2 --warmup 3 --skip-cpu --skip-e2e --skip-batch --skip-extra
 # (profiles/launch_list_snapshot_lj_256atoms_bf16x3.md): the compact form's
-# grouped second product 0.798e9 + 1.753e9, its MN-major third product
-# 1.842e9 + 1.801e9, the FP64 writer 0.006e9 + 3.561e9; the dense-layout
+# grouped second product 0.759e9 + 1.157e9, its MN-major third product
+# 1.541e9 + 1.764e9, the FP64 writer 0.005e9 + 3.561e9; the dense-layout
 # symmetric product (taken where the compact form does not pay) 3.770e9.
-NCU_TRAFFIC = {"mode_product_tc2_p2": 2.551e9, "mode_product_tc2_p3": 3.643e9, "mode_product_tc2_sym": 3.770e9,
-               "ifc3_dense_psi64": 3.567e9}
+NCU_TRAFFIC = {"mode_product_tc2_p2": 1.916e9, "mode_product_tc2_p3": 3.305e9, "mode_product_tc2_sym": 3.770e9,
+               "ifc3_dense_psi64": 3.566e9}
 
 
 def sym_executed_flops(R, F, K, M, split=3):
