@@ -24,7 +24,6 @@ constexpr int PC = 32;  // modes per CTA
 constexpr int PB = 4;   // modes per shared-memory column block
 constexpr int CJ = 8;   // rows per 16-byte store of a BF16 plane
 constexpr int P1C_THREADS = 384;  // compact form: ≥ 3·Kc/2 tasks for neighbourhoods up to 84 atoms
-constexpr int SP = 4;             // compact form: parts of each self-column sum (3·PC·SP = P1C_THREADS tasks)
 
 struct SparseP1Args {
     int N, n, cap, M, mode_lo;
@@ -268,7 +267,6 @@ __global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a
     float* cp = phis + L * (PC + 1);        // pair part [3][6][L], then self part [3][3][L]
     float* cs = cp + 18 * L;
     float* selfres = cp + 27 * L;           // [9][PC]
-    float* selfpart = selfres + 9 * PC;     // [SP][9][PC] partial sums
     const int* nbK = a.nb + (int64_t)K * a.N;
     for (int il = threadIdx.x; il < L; il += blockDim.x) {
         const int sl = il / 3;
@@ -284,28 +282,21 @@ __global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a
         for (int e = threadIdx.x; e < 27 * L / 4; e += blockDim.x) c4[e] = cg[e];
     }
     __syncthreads();
-    // The 9·PC self-column sums (length 3·cnt each) in SP parts over all the
-    // CTA's threads, then combined once below (after the φK rows).
-    {
-        const int len = 3 * cnt, qn = (len + SP - 1) / SP;
-        for (int o = threadIdx.x; o < 3 * PC * SP; o += blockDim.x) {
-            const int pp = o % PC, g = (o / PC) % 3, part = o / (3 * PC);  // kj = g, g+3, g+6
-            const float* c0 = cs + g * L;
-            const float* c1 = cs + (g + 3) * L;
-            const float* c2 = cs + (g + 6) * L;
-            const int i0 = part * qn, i1 = min(len, i0 + qn);
-            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-            for (int il = i0; il < i1; ++il) {
-                const float ph = phis[il * (PC + 1) + pp];
-                s0 = fmaf(c0[il], ph, s0);
-                s1 = fmaf(c1[il], ph, s1);
-                s2 = fmaf(c2[il], ph, s2);
-            }
-            float* out = selfpart + part * 9 * PC;
-            out[g * PC + pp] = s0;
-            out[(g + 3) * PC + pp] = s1;
-            out[(g + 6) * PC + pp] = s2;
+    for (int o = threadIdx.x; o < 3 * PC; o += blockDim.x) {
+        const int pp = o % PC, g = o / PC;  // kj = g, g+3, g+6
+        const float* c0 = cs + g * L;
+        const float* c1 = cs + (g + 3) * L;
+        const float* c2 = cs + (g + 6) * L;
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+        for (int il = 0; il < 3 * cnt; ++il) {
+            const float ph = phis[il * (PC + 1) + pp];
+            s0 = fmaf(c0[il], ph, s0);
+            s1 = fmaf(c1[il], ph, s1);
+            s2 = fmaf(c2[il], ph, s2);
         }
+        selfres[g * PC + pp] = s0;
+        selfres[(g + 3) * PC + pp] = s1;
+        selfres[(g + 6) * PC + pp] = s2;
     }
     // φK rows of this CTA's modes (no dependence on the self sums)
     const int npair = a.Kc / 2;
@@ -315,13 +306,6 @@ __global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a
         const float v0 = j0 < 3 * cnt ? phis[j0 * (PC + 1) + pp] : 0.f;
         const float v1 = j0 + 1 < 3 * cnt ? phis[(j0 + 1) * (PC + 1) + pp] : 0.f;
         store_pair<KIND>(a.pk_hi, a.pk_lo, (int64_t)j0 + (int64_t)a.Kc * ((p0 + pp) + (int64_t)a.M * K), v0, v1);
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < 9 * PC; o += blockDim.x) {
-        float t = selfpart[o];
-#pragma unroll
-        for (int part = 1; part < SP; ++part) t += selfpart[part * 9 * PC + o];
-        selfres[o] = t;
     }
     __syncthreads();
     for (int task = threadIdx.x; task < 3 * npair; task += blockDim.x) {
@@ -408,7 +392,7 @@ namespace fcb {
 
 size_t sparse_p1c_smem_bytes(int cap) {
     const size_t L = 3 * (size_t)cap;
-    return sizeof(float) * (L * (PC + 1) + 27 * L + 9 * PC * (1 + SP));
+    return sizeof(float) * (L * (PC + 1) + 27 * L + 9 * PC);
 }
 
 int sparse_p1c_launch(int kind, int64_t N, int cap, const int* d_nb, const int* d_count, const int* d_self,
