@@ -24,6 +24,7 @@ constexpr int PC = 32;  // modes per CTA
 constexpr int PB = 4;   // modes per shared-memory column block
 constexpr int CJ = 8;   // rows per 16-byte store of a BF16 plane
 constexpr int P1C_THREADS = 384;  // compact form: ≥ 3·Kc/2 tasks for neighbourhoods up to 84 atoms
+constexpr int PSC = PC + 2;       // compact form: row stride of the staged φ rows (8-byte aligned mode pairs)
 
 struct SparseP1Args {
     int N, n, cap, M, mode_lo;
@@ -263,8 +264,8 @@ __global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a
     const int L = 3 * a.cap;
     const int cnt = a.count[K], ss = a.self_slot[K];
     if (cnt > a.cap) return;  // reported by the coefficient kernel; the output is invalid
-    float* phis = sm;                       // [L][PC+1]
-    float* cp = phis + L * (PC + 1);        // pair part [3][6][L], then self part [3][3][L]
+    float* phis = sm;                       // [L][PSC]
+    float* cp = phis + L * PSC;             // pair part [3][6][L], then self part [3][3][L]
     float* cs = cp + 18 * L;
     float* selfres = cp + 27 * L;           // [9][PC]
     const int* nbK = a.nb + (int64_t)K * a.N;
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a
         const int64_t src = live ? (int64_t)(3 * nbK[sl] + il % 3) + (int64_t)a.n * (a.mode_lo + p0) : 0;
 #pragma unroll 8
         for (int pp = 0; pp < PC; ++pp)
-            phis[il * (PC + 1) + pp] = (live && p0 + pp < a.M) ? a.phi[src + (int64_t)a.n * pp] : 0.f;
+            phis[il * PSC + pp] = (live && p0 + pp < a.M) ? a.phi[src + (int64_t)a.n * pp] : 0.f;
     }
     {
         const float4* cg = reinterpret_cast<const float4*>(a.coef + (int64_t)K * 27 * L);
@@ -288,8 +289,31 @@ __global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a
         const float* c1 = cs + (g + 3) * L;
         const float* c2 = cs + (g + 6) * L;
         float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-        for (int il = 0; il < 3 * cnt; ++il) {
-            const float ph = phis[il * (PC + 1) + pp];
+        const int n3 = 3 * cnt;
+        int il = 0;
+        // four rows per step: the coefficient rows as float4 (L is a multiple
+        // of 4), the same summation order as one row at a time
+        for (; il + 4 <= n3; il += 4) {
+            const float4 a0 = *reinterpret_cast<const float4*>(c0 + il);
+            const float4 a1 = *reinterpret_cast<const float4*>(c1 + il);
+            const float4 a2 = *reinterpret_cast<const float4*>(c2 + il);
+            const float* ph = phis + il * PSC + pp;
+            const float f0 = ph[0], f1 = ph[PSC], f2 = ph[2 * PSC], f3 = ph[3 * PSC];
+            s0 = fmaf(a0.x, f0, s0);
+            s1 = fmaf(a1.x, f0, s1);
+            s2 = fmaf(a2.x, f0, s2);
+            s0 = fmaf(a0.y, f1, s0);
+            s1 = fmaf(a1.y, f1, s1);
+            s2 = fmaf(a2.y, f1, s2);
+            s0 = fmaf(a0.z, f2, s0);
+            s1 = fmaf(a1.z, f2, s1);
+            s2 = fmaf(a2.z, f2, s2);
+            s0 = fmaf(a0.w, f3, s0);
+            s1 = fmaf(a1.w, f3, s1);
+            s2 = fmaf(a2.w, f3, s2);
+        }
+        for (; il < n3; ++il) {
+            const float ph = phis[il * PSC + pp];
             s0 = fmaf(c0[il], ph, s0);
             s1 = fmaf(c1[il], ph, s1);
             s2 = fmaf(c2[il], ph, s2);
@@ -303,8 +327,8 @@ __global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a
     for (int it = threadIdx.x; it < PC * npair; it += blockDim.x) {
         const int pp = it / npair, j0 = 2 * (it - pp * npair);
         if (p0 + pp >= a.M) break;
-        const float v0 = j0 < 3 * cnt ? phis[j0 * (PC + 1) + pp] : 0.f;
-        const float v1 = j0 + 1 < 3 * cnt ? phis[(j0 + 1) * (PC + 1) + pp] : 0.f;
+        const float v0 = j0 < 3 * cnt ? phis[j0 * PSC + pp] : 0.f;
+        const float v1 = j0 + 1 < 3 * cnt ? phis[(j0 + 1) * PSC + pp] : 0.f;
         store_pair<KIND>(a.pk_hi, a.pk_lo, (int64_t)j0 + (int64_t)a.Kc * ((p0 + pp) + (int64_t)a.M * K), v0, v1);
     }
     __syncthreads();
@@ -314,34 +338,58 @@ __global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a
         int rowj[2];
         bool self[2], valid[2];
         const float* sres[2];
+        bool pair[2];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int jv = j0 + h, sl = jv / 3, jc = jv - 3 * sl;
             valid[h] = sl < cnt;
             self[h] = sl == ss;
-            const bool pair = valid[h] && !self[h];
-            rowj[h] = pair ? 3 * sl : 3 * ss;
-#pragma unroll
-            for (int t2 = 0; t2 < 6; ++t2) c[h][t2] = pair ? cp[(kc * 6 + t2) * L + jv] : 0.f;
+            pair[h] = valid[h] && !self[h];
+            rowj[h] = pair[h] ? 3 * sl : 3 * ss;
             sres[h] = selfres + (kc * 3 + jc) * PC;
         }
-        const float* yk = phis + 3 * ss * (PC + 1);
+        // both columns' coefficients by one 8-byte load (j0 even, L a multiple of 4)
+#pragma unroll
+        for (int t2 = 0; t2 < 6; ++t2) {
+            const float2 cc = j0 < L ? *reinterpret_cast<const float2*>(cp + (kc * 6 + t2) * L + j0)
+                                     : make_float2(0.f, 0.f);
+            c[0][t2] = pair[0] ? cc.x : 0.f;
+            c[1][t2] = pair[1] ? cc.y : 0.f;
+        }
+        const float* yk = phis + 3 * ss * PSC;
         int64_t off = (int64_t)j0 + (int64_t)a.Kc * (p0 + (int64_t)a.Mp * (3 * K + kc));
-        for (int pp = 0; pp < PC; ++pp, off += a.Kc) {
-            const float y0 = yk[pp], y1 = yk[(PC + 1) + pp], y2 = yk[2 * (PC + 1) + pp];
-            float v[2];
+        // two modes per step: 8-byte shared loads (rows are PSC = PC + 2 floats apart)
+        for (int pp = 0; pp < PC; pp += 2, off += 2 * (int64_t)a.Kc) {
+            const float2 y0 = *reinterpret_cast<const float2*>(yk + pp);
+            const float2 y1 = *reinterpret_cast<const float2*>(yk + PSC + pp);
+            const float2 y2 = *reinterpret_cast<const float2*>(yk + 2 * PSC + pp);
+            float v0[2], v1[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                const float* xj = phis + rowj[h] * (PC + 1) + pp;
-                float s = c[h][0] * xj[0];
-                s = fmaf(c[h][1], xj[PC + 1], s);
-                s = fmaf(c[h][2], xj[2 * (PC + 1)], s);
-                s = fmaf(c[h][3], y0, s);
-                s = fmaf(c[h][4], y1, s);
-                s = fmaf(c[h][5], y2, s);
-                v[h] = !valid[h] ? 0.f : self[h] ? sres[h][pp] : s;
+                const float* xj = phis + rowj[h] * PSC + pp;
+                const float2 x0 = *reinterpret_cast<const float2*>(xj);
+                const float2 x1 = *reinterpret_cast<const float2*>(xj + PSC);
+                const float2 x2 = *reinterpret_cast<const float2*>(xj + 2 * PSC);
+                float s0 = c[h][0] * x0.x, s1 = c[h][0] * x0.y;
+                s0 = fmaf(c[h][1], x1.x, s0);
+                s1 = fmaf(c[h][1], x1.y, s1);
+                s0 = fmaf(c[h][2], x2.x, s0);
+                s1 = fmaf(c[h][2], x2.y, s1);
+                s0 = fmaf(c[h][3], y0.x, s0);
+                s1 = fmaf(c[h][3], y0.y, s1);
+                s0 = fmaf(c[h][4], y1.x, s0);
+                s1 = fmaf(c[h][4], y1.y, s1);
+                s0 = fmaf(c[h][5], y2.x, s0);
+                s1 = fmaf(c[h][5], y2.y, s1);
+                if (self[h]) {  // the self table need not be 8-byte aligned (L may be odd)
+                    s0 = sres[h][pp];
+                    s1 = sres[h][pp + 1];
+                }
+                v0[h] = valid[h] ? s0 : 0.f;
+                v1[h] = valid[h] ? s1 : 0.f;
             }
-            store_pair<KIND>(a.u1_hi, a.u1_lo, off, v[0], v[1]);
+            store_pair<KIND>(a.u1_hi, a.u1_lo, off, v0[0], v0[1]);
+            store_pair<KIND>(a.u1_hi, a.u1_lo, off + a.Kc, v1[0], v1[1]);
         }
     }
 }
@@ -392,7 +440,7 @@ namespace fcb {
 
 size_t sparse_p1c_smem_bytes(int cap) {
     const size_t L = 3 * (size_t)cap;
-    return sizeof(float) * (L * (PC + 1) + 27 * L + 9 * PC);
+    return sizeof(float) * (L * PSC + 27 * L + 9 * PC);
 }
 
 int sparse_p1c_launch(int kind, int64_t N, int cap, const int* d_nb, const int* d_count, const int* d_self,
