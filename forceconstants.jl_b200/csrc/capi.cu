@@ -90,8 +90,9 @@ int check_status(fcb200_context* h, cudaStream_t s) {
         int zero = 0;
         cudaMemcpy(h->d_status, &zero, sizeof(int), cudaMemcpyHostToDevice);
         if (st == DEV_SPARSE_OVERFLOW)
-            return set_error(FCB_ERR_ARG, "a neighbourhood grew past the capacity fixed when the snapshot was added; "
-                                          "set its positions again so that the batch is re-planned");
+            return set_error(FCB_ERR_ARG, "a neighbourhood grew past the capacity fixed in advance (a batch's: set "
+                                          "the snapshot's positions again so that the batch is re-planned; or "
+                                          "fcb200_set_neighbour_capacity's); K3 is invalid");
         if (st == DEV_FD_OVERFLOW)
             return set_error(FCB_ERR_UNSUPPORTED, "finite differences: more than 128 atoms within the SW cutoff of "
                                                   "the displaced atoms");
@@ -310,6 +311,13 @@ int fcb200_synchronize(fcb200_handle h, void* stream) {
 int fcb200_set_wait_limit(fcb200_handle h, int64_t limit_ns) {
     if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
     h->wait_limit_ns = limit_ns > 0 ? (uint64_t)limit_ns : 2000000000ull;
+    return FCB_OK;
+}
+
+int fcb200_set_neighbour_capacity(fcb200_handle h, int cap) {
+    if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
+    if (cap < 0) return set_error(FCB_ERR_ARG, "the neighbour capacity must be >= 0");
+    h->fixed_cap = cap;
     return FCB_OK;
 }
 
@@ -756,7 +764,8 @@ int sparse_snapshot_products(fcb200_context* h, int64_t N, int64_t mode_lo, int6
 // The LJ snapshot with a block-sparse first mode product (split precisions).
 // Needs the largest neighbour count on the host to size the coefficient
 // tables, so it synchronises the stream once (after the neighbour lists; the
-// φ split is already queued behind them).  The FP64 Ψ writer (HBM-bound) runs
+// φ split is already queued behind them), unless the handle has a fixed
+// neighbour capacity (then an overflow is reported by the status word).  The FP64 Ψ writer (HBM-bound) runs
 // on the aux stream beside the tensor-core bound products (the third one in
 // the compact form, the second and third otherwise), with two blocks per SM
 // so that both kernels stay resident on every SM; the caller's stream waits
@@ -783,9 +792,12 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
     int* d_self = d_count + N;
     int* d_max = d_self + N;
     FCB_TRY(lj_neighbour_lists(h, N, d_nb, d_count, d_self, d_max, s));
-    if (!h->h_pinned) FCB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h->h_pinned), 64));
-    FCB_CUDA(cudaMemcpyAsync(h->h_pinned, d_max, sizeof(int), cudaMemcpyDeviceToHost, s));
-    FCB_CUDA(cudaEventRecord(h->ev[0], s));
+    const bool read_back = h->fixed_cap <= 0;
+    if (read_back) {
+        if (!h->h_pinned) FCB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h->h_pinned), 64));
+        FCB_CUDA(cudaMemcpyAsync(h->h_pinned, d_max, sizeof(int), cudaMemcpyDeviceToHost, s));
+        FCB_CUDA(cudaEventRecord(h->ev[0], s));
+    }
     FCB_TRY(split_phi(h, kind, d_phi, n, s));
     const bool host64 = psi_out && !is_device_ptr(psi_out);
     double* d_psi64 = psi_out;
@@ -801,8 +813,11 @@ int snapshot_lj_sparse(fcb200_context* h, const double* d_pos, int64_t N, const 
         out.psi64 = d_psi64;
         FCB_TRY(ifc3_dense_write(h, N, tol, d_m, out, s));
     }
-    FCB_CUDA(cudaEventSynchronize(h->ev[0]));
-    int cap = h->h_pinned[0];
+    int cap = h->fixed_cap;
+    if (read_back) {
+        FCB_CUDA(cudaEventSynchronize(h->ev[0]));
+        cap = h->h_pinned[0];
+    }
     cap = (cap + 3) / 4 * 4;  // table stride: a multiple of 4 floats per component
     // The per-atom tables of the sparse form must fit in shared memory; if they
     // do not, the dense path runs (and writes the FP64 Ψ again).

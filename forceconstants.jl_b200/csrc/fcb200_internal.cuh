@@ -63,6 +63,7 @@ struct fcb200_context {
     int sm_count = 0;
     int* d_status = nullptr;        // device status word (bounded-wait failures)
     uint64_t wait_limit_ns = 2000000000ull;  // limit of the tensor-core kernels' mbarrier waits
+    int fixed_cap = 0;  // > 0: the sparse snapshot path's neighbour capacity, no host read-back
     int* h_pinned = nullptr;        // small pinned host buffer for counts read back during a call
     // assembly scratch
     fcb::Buf pos, box, masses;      // staged inputs

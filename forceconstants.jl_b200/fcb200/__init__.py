@@ -3,12 +3,14 @@
 Host-side mirror of the ForceConstants.jl API for its dense IFC3 + mcc3 path,
 calling the C ABI of ``libfcb200.so`` (``include/fcb200.h``).
 """
+from .batch import SnapshotBatch, trajectory_k3
 from .crystals import FCC, Diamond, displaced
 from .ifc import (asr_satisfied, dynamical_matrix, get_modes, mass_weight_third_order_, second_order,
                   second_order_, third_order, third_order_)
 from .finite_diff import third_order_fd, third_order_finite_diff_eng
 from .io import load_third_order_txt, parse_xyz, save_second_order, save_third_order
-from .mcc import mcc3, mcc3_, mcc3_tens_opt, mcc3_window, packed_k3_count, snapshot_lj, unpack_k3
+from .mcc import (mcc3, mcc3_, mcc3_tens_opt, mcc3_window, packed_k3_count, set_neighbour_capacity, snapshot_lj,
+                  unpack_k3)
 from .types import (LJ, AnalyticalCalculator, AutoDiffCalculator, DenseForceConstants, FiniteDiffCalculator,
                     PairPotential, Potential,
                     StillingerWeberSilicon, SuperCellSystem, ThreeBodyPotential, energy_unit, length_unit, masses,
@@ -21,5 +23,6 @@ __all__ = [
     "PairPotential", "Potential", "StillingerWeberSilicon", "SuperCellSystem", "ThreeBodyPotential",
     "energy_unit", "length_unit", "masses", "n_atoms", "positions", "parse_xyz", "save_third_order",
     "save_second_order", "load_third_order_txt", "FiniteDiffCalculator", "third_order_fd",
-    "third_order_finite_diff_eng",
+    "third_order_finite_diff_eng", "SnapshotBatch", "trajectory_k3",
+    "set_neighbour_capacity",
 ]

@@ -46,6 +46,7 @@ SIGNATURES = {
     "fcb200_trim": (_I, [_P]),
     "fcb200_synchronize": (_I, [_P, _P]),
     "fcb200_set_wait_limit": (_I, [_P, _I64]),
+    "fcb200_set_neighbour_capacity": (_I, [_P, _I]),
     "fcb200_third_order_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _D, _P, _P, _P, _I, _P]),
     "fcb200_mass_weight3": (_I, [_P, _P, _P, _I64, _P]),
     "fcb200_second_order_lj": (_I, [_P, _P, _I64, _P, _D, _D, _D, _D, _P, _P, _P]),

@@ -107,6 +107,15 @@ def snapshot_lj(sys, pot, calc, phi, precision: str = "bf16x3", modes=None, psi_
     return psi_out, k3_out
 
 
+def set_neighbour_capacity(cap: int, device: int = 0):
+    """Fixes the neighbour capacity of the block-sparse snapshot path on this
+    device's handle (fcb200_set_neighbour_capacity): 0 restores the default
+    (one read-back of the largest neighbour count per snapshot_lj call);
+    cap > 0 removes that read-back, so that the call can be captured in a CUDA
+    graph, and an atom with more neighbours makes the next synchronize raise."""
+    _lib.check(_lib.lib().fcb200_set_neighbour_capacity(_lib.handle(device), int(cap)))
+
+
 def packed_k3_count(M: int) -> int:
     """Entries K3[p,q,s] with p <= q <= s of an M-mode K3 (FCB_K3_PACKED)."""
     return M * (M + 1) * (M + 2) // 6

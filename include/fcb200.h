@@ -93,6 +93,17 @@ int fcb200_synchronize(fcb200_handle h, void* stream);
  * limit_ns <= 0 restores the default of 2 s. */
 int fcb200_set_wait_limit(fcb200_handle h, int64_t limit_ns);
 
+/* Neighbour capacity of the block-sparse snapshot path (no counterpart in the
+ * reference).  cap = 0 (the default): fcb200_snapshot_lj reads the largest
+ * neighbour count back to the host once per call (one synchronisation of the
+ * stream, after the neighbour lists) and sizes its tables by it.  cap > 0: the
+ * tables are sized for `cap` neighbours per atom (rounded up to a multiple of
+ * 4), the call does not synchronise (so it can be captured in a CUDA graph
+ * after one uncaptured call has sized the handle's scratch), and an atom with
+ * more neighbours makes the next fcb200_synchronize report FCB_ERR_ARG with
+ * K3 invalid (the FP64 Ψ is still written).  cap < 0 is FCB_ERR_ARG. */
+int fcb200_set_neighbour_capacity(fcb200_handle h, int cap);
+
 /*
  * Dense third-order IFCs of a pair Lennard-Jones system with the analytical
  * calculator.  Replaces

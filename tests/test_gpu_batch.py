@@ -61,6 +61,37 @@ def test_batch_matches_single_snapshots(fcb, oracle, cuda_device, precision):
     b.close()
 
 
+def test_trajectory_k3_matches_single_snapshots(fcb, oracle, cuda_device, tmp_path):
+    """An xyz trajectory (io.jl:319-353's frames) through trajectory_k3 in
+    groups of two frames: every frame's K3 equals fcb200_snapshot_lj on the
+    same positions bit for bit, the last group holding one frame only."""
+    import torch
+    from fcb200.batch import trajectory_k3
+    pot = fcb.LJ(AR["sigma"], AR["eps"], AR["r_cut"])
+    calc = fcb.AnalyticalCalculator(1e-12, AR["r_cut"])
+    base = fcc_system((3, 3, 3))
+    frames = [fcb.displaced(base, 0.03, 200 + t) for t in range(5)]
+    path = tmp_path / "traj.xyz"
+    with open(path, "w") as f:
+        for t, s in enumerate(frames):
+            f.write(f"{s.n_atoms}\nTimestep: {t}\n")
+            f.write("".join(f"{i + 1} {x!r} {y!r} {z!r}\n" for i, (x, y, z) in enumerate(s.positions)))
+    phi = _phi(oracle, base)                      # modes of the perfect lattice, shared by every frame
+    seen = []
+    got = trajectory_k3(str(path), base.n_atoms, 6, base.box_sizes, base.masses, pot, calc, phi,
+                        frames_per_batch=2)
+    trajectory_k3(str(path), base.n_atoms, 6, base.box_sizes, base.masses, pot, calc, phi, frames_per_batch=2,
+                  on_frame=lambda t, ids, k3: seen.append((t, ids.tolist(), k3.cpu().numpy())))
+    assert len(got) == 5 and [t for t, _, _ in seen] == [0, 1, 2, 3, 4]   # the sixth frame is not in the file
+    d_phi = torch.from_numpy(phi).to(cuda_device)
+    for s, k, (_, ids, k2) in zip(frames, got, seen):
+        _, ref = fcb.snapshot_lj(s, pot, calc, d_phi, precision="bf16x3")
+        torch.cuda.synchronize()
+        ref = ref.cpu().numpy()
+        assert ids == list(range(1, s.n_atoms + 1))
+        assert np.array_equal(k, ref) and np.array_equal(k2, ref)
+
+
 def test_batch_admission_refuses_oversize(fcb, cuda_device):
     from fcb200 import _lib
     from fcb200.batch import SnapshotBatch
