@@ -100,8 +100,9 @@ int fcb200_set_wait_limit(fcb200_handle h, int64_t limit_ns);
  * tables are sized for `cap` neighbours per atom (rounded up to a multiple of
  * 4), the call does not synchronise (so it can be captured in a CUDA graph
  * after one uncaptured call has sized the handle's scratch), and an atom with
- * more neighbours makes the next fcb200_synchronize report FCB_ERR_ARG with
- * K3 invalid (the FP64 Ψ is still written).  cap < 0 is FCB_ERR_ARG. */
+ * more neighbours is reported as FCB_ERR_ARG, K3 invalid (the FP64 Ψ is still
+ * written): by the call itself when it synchronises (host positions or host
+ * outputs), else by the next fcb200_synchronize.  cap < 0 is FCB_ERR_ARG. */
 int fcb200_set_neighbour_capacity(fcb200_handle h, int cap);
 
 /*

@@ -75,7 +75,7 @@ def test_trajectory_k3_matches_single_snapshots(fcb, oracle, cuda_device, tmp_pa
     with open(path, "w") as f:
         for t, s in enumerate(frames):
             f.write(f"{s.n_atoms}\nTimestep: {t}\n")
-            f.write("".join(f"{i + 1} {x!r} {y!r} {z!r}\n" for i, (x, y, z) in enumerate(s.positions)))
+            f.write("".join(f"{i + 1} {x!r} {y!r} {z!r}\n" for i, (x, y, z) in enumerate(s.positions.tolist())))
     phi = _phi(oracle, base)                      # modes of the perfect lattice, shared by every frame
     seen = []
     got = trajectory_k3(str(path), base.n_atoms, 6, base.box_sizes, base.masses, pot, calc, phi,

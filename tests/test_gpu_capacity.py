@@ -10,8 +10,9 @@ host once per call.  With a capacity fixed on the handle it does not, so:
 * the call can be captured in a CUDA graph, after one uncaptured call has
   sized the handle's scratch, and every replay rewrites the same K3;
 * a capacity below the largest neighbourhood (8 slots against 79 neighbours
-  with the atom itself) makes the next fcb200_synchronize report FCB_ERR_ARG,
-  and the handle then runs a normal call again.
+  with the atom itself) is reported as FCB_ERR_ARG (by the call itself, which
+  synchronises when its positions are on the host), and the handle then runs a
+  normal call again.
 """
 import numpy as np
 import pytest
@@ -102,8 +103,8 @@ def test_capacity_overflow_reported_and_handle_recovers(fcb, cuda_device, cell):
     k3_ref = k3.clone()
     try:
         fcb.set_neighbour_capacity(8)
-        _run(fcb, s, d_phi, psi, k3)
         with pytest.raises(_lib.FCB200Error) as e:
+            _run(fcb, s, d_phi, psi, k3)         # host positions: the call synchronises and reports
             _lib.check(L.fcb200_synchronize(h, 0))
         assert e.value.code == _lib.FCB_ERR_ARG
     finally:
