@@ -262,9 +262,10 @@ int sparse_p1c_launch(int kind, int64_t N, int cap, const int* d_nb, const int* 
 // Whether mode products run on the 2-CTA tile (mode_product_tc.cu).
 bool tc_pair_enabled();
 // Shapes of the compact sparse products: modes padded to whole 256-row blocks,
-// neighbourhood rows to a multiple of 8.
+// neighbourhood rows to a multiple of 16 (the first product stores 16 rows
+// of a mode as one 32-byte sector per plane).
 inline int64_t compact_Mp(int64_t M) { return (M + 255) / 256 * 256; }
-inline int64_t compact_Kc(int cap) { return (3 * (int64_t)cap + 7) / 8 * 8; }
+inline int64_t compact_Kc(int cap) { return (3 * (int64_t)cap + 15) / 16 * 16; }
 // The compact form pays when its grouped second product and padded third
 // product execute at least 10 % fewer tile flops than the dense-K pair.
 inline bool compact_pays(int64_t n, int64_t M, int cap) {

@@ -23,8 +23,10 @@ namespace {
 constexpr int PC = 32;  // modes per CTA
 constexpr int PB = 4;   // modes per shared-memory column block
 constexpr int CJ = 8;   // rows per 16-byte store of a BF16 plane
-constexpr int P1C_THREADS = 384;  // compact form: ≥ 3·Kc/2 tasks for neighbourhoods up to 84 atoms
-constexpr int PSC = PC + 2;       // compact form: row stride of the staged φ rows (8-byte aligned mode pairs)
+constexpr int P1T_MODES = 64;     // compact form: modes per CTA (one per thread of a warp pair)
+constexpr int P1T_THREADS = 256;  // compact form: 8 warps
+constexpr int P1T_J = 16;         // compact form: rows j' per chunk (one 32-byte sector per BF16 plane)
+constexpr int P1T_LD = P1T_MODES + 1;  // compact form: row stride of the staged φ rows (odd: no bank conflicts)
 
 struct SparseP1Args {
     int N, n, cap, M, mode_lo;
@@ -223,10 +225,7 @@ __global__ void __launch_bounds__(256) sparse_p1_kernel(SparseP1Args a) {
 // and, as the second product's per-atom operand, the same rows of φ:
 //     φK[j' + Kc·(q + M·K)] = φ[3·nbr(K)[slot] + jc, q].
 // The second product is then a grouped GEMM over the atoms with Kc (about
-// 3·|nbr|) instead of n terms.  One CTA per (atom K, PC modes); one thread per
-// (kc, pair of rows j') walks the modes with its 12 coefficients in registers;
-// a warp stores 128 contiguous bytes per plane.  Rows p ≥ M (up to Mp) are
-// written as zeros.
+// 3·|nbr|) instead of n terms.
 struct SparseP1cArgs {
     int N, n, cap, M, Mp, Kc, mode_lo;
     const int* nb;
@@ -240,42 +239,155 @@ struct SparseP1cArgs {
     void* pk_lo;
 };
 
+// Packed FP32 pairs (Blackwell's f32x2 mul / fma: two IEEE operations per
+// instruction, each rounded as mulf / fmaf would round it).
+__device__ __forceinline__ uint64_t f2u(float2 v) { return *reinterpret_cast<const uint64_t*>(&v); }
+__device__ __forceinline__ float2 u2f(uint64_t v) { return *reinterpret_cast<const float2*>(&v); }
+
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2u(a)), "l"(f2u(b)));
+    return u2f(d);
+}
+
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2u(a)), "l"(f2u(b)), "l"(f2u(c)));
+    return u2f(d);
+}
+
+// 32 bytes in one 256-bit store (a whole L2 sector per lane).
+__device__ __forceinline__ void st_v8(void* p, const uint32_t (&v)[8]) {
+    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(v[0]), "r"(v[1]),
+                 "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+                 : "memory");
+}
+
+// Split 16 consecutive values into the hi/lo planes at element offset `off`
+// (a multiple of 16): 32 bytes per BF16 plane, 64 per TF32 plane.
 template <int KIND>
-__device__ __forceinline__ void store_pair(void* hi, void* lo, int64_t off, float v0, float v1) {
+__device__ __forceinline__ void store_chunk16(void* hi, void* lo, int64_t off, const float (&v)[P1T_J]) {
     if constexpr (KIND == 1) {
-        const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
-        const __nv_bfloat162 l = __floats2bfloat162_rn(v0 - __low2float(h), v1 - __high2float(h));
-        *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(hi) + off) = h;
-        *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(lo) + off) = l;
+        uint32_t h[8], l[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const __nv_bfloat162 hb = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+            const __nv_bfloat162 lb =
+                __floats2bfloat162_rn(v[2 * i] - __low2float(hb), v[2 * i + 1] - __high2float(hb));
+            h[i] = *reinterpret_cast<const uint32_t*>(&hb);
+            l[i] = *reinterpret_cast<const uint32_t*>(&lb);
+        }
+        st_v8(static_cast<__nv_bfloat16*>(hi) + off, h);
+        st_v8(static_cast<__nv_bfloat16*>(lo) + off, l);
     } else {
-        uint32_t b0, b1;
-        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b0) : "f"(v0));
-        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b1) : "f"(v1));
-        const float h0 = __uint_as_float(b0), h1 = __uint_as_float(b1);
-        *reinterpret_cast<float2*>(static_cast<float*>(hi) + off) = make_float2(h0, h1);
-        *reinterpret_cast<float2*>(static_cast<float*>(lo) + off) = make_float2(v0 - h0, v1 - h1);
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            uint32_t h[8], l[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                uint32_t b;
+                asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b) : "f"(v[8 * half + i]));
+                h[i] = b;
+                l[i] = __float_as_uint(v[8 * half + i] - __uint_as_float(b));
+            }
+            st_v8(static_cast<float*>(hi) + off + 8 * half, h);
+            st_v8(static_cast<float*>(lo) + off + 8 * half, l);
+        }
     }
 }
 
+// One chunk of 16 rows j' = j0..j0+15 (j0 % 16 == 0, R = j0 % 3) of the three
+// columns k = 3K + kc for this thread's mode: x[s][t] are the staged φ values
+// of the slots j0/3 .. j0/3 + 5 (DOF t), y[t] those of atom K itself.  Every
+// entry is c0·x0 then five fused multiply-adds in the order of the reference
+// contraction's terms (the ASR self rows come from `self`).
+template <int KIND, int R>
+__device__ __forceinline__ void p1t_chunk(const float* __restrict__ cp, int L, int j0, int n3, int ss,
+                                          const float (&x)[6][3], const float (&y)[3],
+                                          const float* __restrict__ selfp, void* hi, void* lo, int64_t off,
+                                          int64_t kc_stride) {
+    // operands of the row pairs (j0 + 2i, j0 + 2i + 1): slot of row j0 + jj is (R + jj) / 3
+    float2 xs[3][8];
+#pragma unroll
+    for (int t = 0; t < 3; ++t)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) xs[t][i] = make_float2(x[(R + 2 * i) / 3][t], x[(R + 2 * i + 1) / 3][t]);
+    const float2 y0 = make_float2(y[0], y[0]), y1 = make_float2(y[1], y[1]), y2 = make_float2(y[2], y[2]);
+    const int sl0 = j0 / 3;
+    const bool has_self = 3 * ss + 2 >= j0 && 3 * ss <= j0 + P1T_J - 1;
+#pragma unroll
+    for (int kc = 0; kc < 3; ++kc) {
+        float2 acc[8];
+        const float* c = cp + (int64_t)(kc * 6) * L + j0;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 cq = *reinterpret_cast<const float4*>(c + t * L + 4 * q);
+                const float2 ca = make_float2(cq.x, cq.y), cb = make_float2(cq.z, cq.w);
+                const float2 za = t < 3 ? xs[t < 3 ? t : 0][2 * q] : t == 3 ? y0 : t == 4 ? y1 : y2;
+                const float2 zb = t < 3 ? xs[t < 3 ? t : 0][2 * q + 1] : t == 3 ? y0 : t == 4 ? y1 : y2;
+                if (t == 0) {
+                    acc[2 * q] = mul2(ca, za);
+                    acc[2 * q + 1] = mul2(cb, zb);
+                } else {
+                    acc[2 * q] = fma2(ca, za, acc[2 * q]);
+                    acc[2 * q + 1] = fma2(cb, zb, acc[2 * q + 1]);
+                }
+            }
+        }
+        float v[P1T_J];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            v[2 * i] = acc[i].x;
+            v[2 * i + 1] = acc[i].y;
+        }
+        // the self slot's rows: the ASR sums (its pair coefficients are zero)
+        if (has_self) {
+#pragma unroll
+            for (int jj = 0; jj < P1T_J; ++jj)
+                if ((R + jj) / 3 + sl0 == ss) v[jj] = selfp[(kc * 3 + (R + jj) % 3) * P1T_MODES];
+        }
+        // rows past the neighbourhood are exact zeros
+        if (j0 + P1T_J > n3) {
+#pragma unroll
+            for (int jj = 0; jj < P1T_J; ++jj)
+                if (j0 + jj >= n3) v[jj] = 0.f;
+        }
+        store_chunk16<KIND>(hi, lo, off + kc * kc_stride, v);
+    }
+}
+
+// One CTA per (atom K, P1T_MODES modes), one thread per mode: a thread walks
+// the rows j' of K's neighbourhood in chunks of 16 for all three columns
+// 3K + kc at once, with the staged φ values of its mode in registers and the
+// coefficient rows read as shared-memory broadcasts, and stores each chunk of
+// 16 rows as one 32-byte sector per BF16 plane (its mode's rows are contiguous
+// in U1c).
+// Warps 0-5 first form the ASR self sums of column kc = warp / 2 (in the
+// reference's term order), while warps 6-7 write the φK rows; after one
+// barrier the chunks go round-robin to the four warp pairs.  Rows p ≥ M (up
+// to Mp) are written as zeros.
 template <int KIND>
-__global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a) {
+__global__ void __launch_bounds__(P1T_THREADS, 2) sparse_p1t_kernel(SparseP1cArgs a) {
     extern __shared__ float sm[];
-    const int K = blockIdx.y, p0 = blockIdx.x * PC;
+    const int K = blockIdx.y, p0 = blockIdx.x * P1T_MODES;
     const int L = 3 * a.cap;
     const int cnt = a.count[K], ss = a.self_slot[K];
     if (cnt > a.cap) return;  // reported by the coefficient kernel; the output is invalid
-    float* phis = sm;                       // [L][PSC]
-    float* cp = phis + L * PSC;             // pair part [3][6][L], then self part [3][3][L]
+    const int n3 = 3 * cnt;
+    float* phis = sm;                          // [L][P1T_LD], mode fastest
+    float* cp = phis + L * P1T_LD;             // pair part [kc][t][L], then self part [kc][jc][L]
     float* cs = cp + 18 * L;
-    float* selfres = cp + 27 * L;           // [9][PC]
+    float* selfres = cp + 27 * L;              // [kc][jc][P1T_MODES]
     const int* nbK = a.nb + (int64_t)K * a.N;
     for (int il = threadIdx.x; il < L; il += blockDim.x) {
         const int sl = il / 3;
         const bool live = sl < cnt;
-        const int64_t src = live ? (int64_t)(3 * nbK[sl] + il % 3) + (int64_t)a.n * (a.mode_lo + p0) : 0;
+        const float* src = a.phi + (live ? (int64_t)(3 * nbK[sl] + il % 3) + (int64_t)a.n * (a.mode_lo + p0) : 0);
 #pragma unroll 8
-        for (int pp = 0; pp < PC; ++pp)
-            phis[il * PSC + pp] = (live && p0 + pp < a.M) ? a.phi[src + (int64_t)a.n * pp] : 0.f;
+        for (int pp = 0; pp < P1T_MODES; ++pp)
+            phis[il * P1T_LD + pp] = (live && p0 + pp < a.M) ? src[(int64_t)a.n * pp] : 0.f;
     }
     {
         const float4* cg = reinterpret_cast<const float4*>(a.coef + (int64_t)K * 27 * L);
@@ -283,22 +395,23 @@ __global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a
         for (int e = threadIdx.x; e < 27 * L / 4; e += blockDim.x) c4[e] = cg[e];
     }
     __syncthreads();
-    for (int o = threadIdx.x; o < 3 * PC; o += blockDim.x) {
-        const int pp = o % PC, g = o / PC;  // kj = g, g+3, g+6
-        const float* c0 = cs + g * L;
-        const float* c1 = cs + (g + 3) * L;
-        const float* c2 = cs + (g + 6) * L;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = (warp & 1) * 32 + lane;      // this thread's mode (p0 + p)
+    const int npk = a.Kc / P1T_J;              // chunks of 16 rows
+    if (warp < 6) {
+        // self sums of column kc: Σ_il cs[kc][jc][il] · φ[il, p], il ascending
+        const int kc = warp >> 1;
+        const float* c0 = cs + (kc * 3) * L;
+        const float* c1 = c0 + L;
+        const float* c2 = c1 + L;
         float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-        const int n3 = 3 * cnt;
         int il = 0;
-        // four rows per step: the coefficient rows as float4 (L is a multiple
-        // of 4), the same summation order as one row at a time
         for (; il + 4 <= n3; il += 4) {
             const float4 a0 = *reinterpret_cast<const float4*>(c0 + il);
             const float4 a1 = *reinterpret_cast<const float4*>(c1 + il);
             const float4 a2 = *reinterpret_cast<const float4*>(c2 + il);
-            const float* ph = phis + il * PSC + pp;
-            const float f0 = ph[0], f1 = ph[PSC], f2 = ph[2 * PSC], f3 = ph[3 * PSC];
+            const float* ph = phis + il * P1T_LD + p;
+            const float f0 = ph[0], f1 = ph[P1T_LD], f2 = ph[2 * P1T_LD], f3 = ph[3 * P1T_LD];
             s0 = fmaf(a0.x, f0, s0);
             s1 = fmaf(a1.x, f0, s1);
             s2 = fmaf(a2.x, f0, s2);
@@ -313,83 +426,55 @@ __global__ void __launch_bounds__(P1C_THREADS) sparse_p1c_kernel(SparseP1cArgs a
             s2 = fmaf(a2.w, f3, s2);
         }
         for (; il < n3; ++il) {
-            const float ph = phis[il * PSC + pp];
+            const float ph = phis[il * P1T_LD + p];
             s0 = fmaf(c0[il], ph, s0);
             s1 = fmaf(c1[il], ph, s1);
             s2 = fmaf(c2[il], ph, s2);
         }
-        selfres[g * PC + pp] = s0;
-        selfres[(g + 3) * PC + pp] = s1;
-        selfres[(g + 6) * PC + pp] = s2;
-    }
-    // φK rows of this CTA's modes (no dependence on the self sums)
-    const int npair = a.Kc / 2;
-    for (int it = threadIdx.x; it < PC * npair; it += blockDim.x) {
-        const int pp = it / npair, j0 = 2 * (it - pp * npair);
-        if (p0 + pp >= a.M) break;
-        const float v0 = j0 < 3 * cnt ? phis[j0 * PSC + pp] : 0.f;
-        const float v1 = j0 + 1 < 3 * cnt ? phis[(j0 + 1) * PSC + pp] : 0.f;
-        store_pair<KIND>(a.pk_hi, a.pk_lo, (int64_t)j0 + (int64_t)a.Kc * ((p0 + pp) + (int64_t)a.M * K), v0, v1);
+        selfres[(kc * 3 + 0) * P1T_MODES + p] = s0;
+        selfres[(kc * 3 + 1) * P1T_MODES + p] = s1;
+        selfres[(kc * 3 + 2) * P1T_MODES + p] = s2;
+    } else if (p0 + p < a.M) {
+        // φK rows of this mode: φK[j' + Kc·(q + M·K)], zero past the neighbourhood
+        const int64_t base = (int64_t)a.Kc * ((p0 + p) + (int64_t)a.M * K);
+        for (int ck = 0; ck < npk; ++ck) {
+            float v[P1T_J];
+#pragma unroll
+            for (int jj = 0; jj < P1T_J; ++jj) {
+                const int j = ck * P1T_J + jj;
+                v[jj] = j < n3 ? phis[j * P1T_LD + p] : 0.f;
+            }
+            store_chunk16<KIND>(a.pk_hi, a.pk_lo, base + ck * P1T_J, v);
+        }
     }
     __syncthreads();
-    for (int task = threadIdx.x; task < 3 * npair; task += blockDim.x) {
-        const int kc = task / npair, j0 = 2 * (task - kc * npair);
-        float c[2][6];
-        int rowj[2];
-        bool self[2], valid[2];
-        const float* sres[2];
-        bool pair[2];
+    float y[3];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int jv = j0 + h, sl = jv / 3, jc = jv - 3 * sl;
-            valid[h] = sl < cnt;
-            self[h] = sl == ss;
-            pair[h] = valid[h] && !self[h];
-            rowj[h] = pair[h] ? 3 * sl : 3 * ss;
-            sres[h] = selfres + (kc * 3 + jc) * PC;
-        }
-        // both columns' coefficients by one 8-byte load (j0 even, L a multiple of 4)
+    for (int t = 0; t < 3; ++t) y[t] = phis[(3 * ss + t) * P1T_LD + p];
+    const int64_t off0 = (int64_t)a.Kc * ((p0 + p) + (int64_t)a.Mp * (3 * K));
+    const int64_t kc_stride = (int64_t)a.Kc * a.Mp;
+    const float* selfp = selfres + p;
+    for (int ck = warp >> 1; ck < npk; ck += P1T_THREADS / 64) {
+        const int j0 = ck * P1T_J;
+        const int sl0 = j0 / 3;
+        float x[6][3];
 #pragma unroll
-        for (int t2 = 0; t2 < 6; ++t2) {
-            const float2 cc = j0 < L ? *reinterpret_cast<const float2*>(cp + (kc * 6 + t2) * L + j0)
-                                     : make_float2(0.f, 0.f);
-            c[0][t2] = pair[0] ? cc.x : 0.f;
-            c[1][t2] = pair[1] ? cc.y : 0.f;
-        }
-        const float* yk = phis + 3 * ss * PSC;
-        int64_t off = (int64_t)j0 + (int64_t)a.Kc * (p0 + (int64_t)a.Mp * (3 * K + kc));
-        // two modes per step: 8-byte shared loads (rows are PSC = PC + 2 floats apart)
-        for (int pp = 0; pp < PC; pp += 2, off += 2 * (int64_t)a.Kc) {
-            const float2 y0 = *reinterpret_cast<const float2*>(yk + pp);
-            const float2 y1 = *reinterpret_cast<const float2*>(yk + PSC + pp);
-            const float2 y2 = *reinterpret_cast<const float2*>(yk + 2 * PSC + pp);
-            float v0[2], v1[2];
+        for (int s = 0; s < 6; ++s)
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const float* xj = phis + rowj[h] * PSC + pp;
-                const float2 x0 = *reinterpret_cast<const float2*>(xj);
-                const float2 x1 = *reinterpret_cast<const float2*>(xj + PSC);
-                const float2 x2 = *reinterpret_cast<const float2*>(xj + 2 * PSC);
-                float s0 = c[h][0] * x0.x, s1 = c[h][0] * x0.y;
-                s0 = fmaf(c[h][1], x1.x, s0);
-                s1 = fmaf(c[h][1], x1.y, s1);
-                s0 = fmaf(c[h][2], x2.x, s0);
-                s1 = fmaf(c[h][2], x2.y, s1);
-                s0 = fmaf(c[h][3], y0.x, s0);
-                s1 = fmaf(c[h][3], y0.y, s1);
-                s0 = fmaf(c[h][4], y1.x, s0);
-                s1 = fmaf(c[h][4], y1.y, s1);
-                s0 = fmaf(c[h][5], y2.x, s0);
-                s1 = fmaf(c[h][5], y2.y, s1);
-                if (self[h]) {  // the self table need not be 8-byte aligned (L may be odd)
-                    s0 = sres[h][pp];
-                    s1 = sres[h][pp + 1];
-                }
-                v0[h] = valid[h] ? s0 : 0.f;
-                v1[h] = valid[h] ? s1 : 0.f;
+            for (int t = 0; t < 3; ++t) {
+                const int row = 3 * (sl0 + s) + t;
+                x[s][t] = row < L ? phis[row * P1T_LD + p] : 0.f;
             }
-            store_pair<KIND>(a.u1_hi, a.u1_lo, off, v0[0], v0[1]);
-            store_pair<KIND>(a.u1_hi, a.u1_lo, off + a.Kc, v1[0], v1[1]);
+        switch (j0 % 3) {
+            case 0:
+                p1t_chunk<KIND, 0>(cp, L, j0, n3, ss, x, y, selfp, a.u1_hi, a.u1_lo, off0 + j0, kc_stride);
+                break;
+            case 1:
+                p1t_chunk<KIND, 1>(cp, L, j0, n3, ss, x, y, selfp, a.u1_hi, a.u1_lo, off0 + j0, kc_stride);
+                break;
+            default:
+                p1t_chunk<KIND, 2>(cp, L, j0, n3, ss, x, y, selfp, a.u1_hi, a.u1_lo, off0 + j0, kc_stride);
+                break;
         }
     }
 }
@@ -440,7 +525,7 @@ namespace fcb {
 
 size_t sparse_p1c_smem_bytes(int cap) {
     const size_t L = 3 * (size_t)cap;
-    return sizeof(float) * (L * PSC + 27 * L + 9 * PC);
+    return sizeof(float) * (L * P1T_LD + 27 * L + 9 * P1T_MODES);
 }
 
 int sparse_p1c_launch(int kind, int64_t N, int cap, const int* d_nb, const int* d_count, const int* d_self,
@@ -464,13 +549,13 @@ int sparse_p1c_launch(int kind, int64_t N, int cap, const int* d_nb, const int* 
     a.pk_hi = pk_hi;
     a.pk_lo = pk_lo;
     const size_t smem = sparse_p1c_smem_bytes(cap);
-    const dim3 grid((unsigned)(Mp / PC), (unsigned)N);
+    const dim3 grid((unsigned)(Mp / P1T_MODES), (unsigned)N);
     if (kind == 1) {
-        FCB_CUDA(cudaFuncSetAttribute(sparse_p1c_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        sparse_p1c_kernel<1><<<grid, P1C_THREADS, smem, s>>>(a);
+        FCB_CUDA(cudaFuncSetAttribute(sparse_p1t_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sparse_p1t_kernel<1><<<grid, P1T_THREADS, smem, s>>>(a);
     } else {
-        FCB_CUDA(cudaFuncSetAttribute(sparse_p1c_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        sparse_p1c_kernel<2><<<grid, P1C_THREADS, smem, s>>>(a);
+        FCB_CUDA(cudaFuncSetAttribute(sparse_p1t_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sparse_p1t_kernel<2><<<grid, P1T_THREADS, smem, s>>>(a);
     }
     FCB_CUDA(cudaGetLastError());
     return FCB_OK;
