@@ -42,7 +42,7 @@ size_t snapshot_footprint(int64_t N, int precision, int cap) {
     const size_t np = (size_t)pad_for(kind, n);
     if (cap > 0) {  // U1, U2 planes, φ planes, coefficient tables, neighbour lists
         const size_t tables = sizeof(float) * (size_t)N * 27 * 3 * cap + sizeof(int) * (size_t)(N * N + 2 * N + 1);
-        if (tc_pair_enabled() && compact_pays(n, n, cap)) {  // compact U1, per-atom φ rows, padded U2
+        if (tc_pair_enabled() && compact_pays(n, n, cap) && sparse_p1c_smem_bytes(cap) <= 227 * 1024) {  // compact U1, per-atom φ rows, padded U2
             const size_t Mp = (size_t)compact_Mp(n), Kc = (size_t)compact_Kc(cap);
             return pair + tables + 2 * esz * (Mp * n * Kc + (size_t)N * n * Kc + Mp * n * n + np * n);
         }

@@ -722,7 +722,9 @@ int compact_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, i
     phase_mark(h, s, 4);
     FCB_TRY(h->u2_hi.ensure(esz * Mp * n * M));
     FCB_TRY(h->u2_lo.ensure(esz * Mp * n * M));
-    ModeProduct p2{Mp * n, Kc, M, Kc, Kc, Mp, Mp, Mp * n};
+    ModeProduct p2{Mp * n, Kc, M, Mp, Kc, Mp, Mp, Mp * n};
+    p2.a_mn = true;        // U1c is stored mode-fastest: U1c[p + Mp·(j' + Kc·k)]
+    p2.lda_z = Mp * Kc;
     p2.sym_inner = true;
     p2.inner_upper = true;  // U2 tiles with p / 256 <= q / 256 only: all the third product reads
     p2.b_group = 3 * Mp;
@@ -750,7 +752,7 @@ template <class Hook>
 int sparse_snapshot_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, int kind, int cap,
                              const int* d_nb, const int* d_count, const int* d_self, double tol, const double* d_m,
                              const float* d_phi, float* d_k3, cudaStream_t s, Hook hook, bool packed = false) {
-    if (tc_pair_enabled() && compact_pays(3 * N, M, cap))
+    if (tc_pair_enabled() && compact_pays(3 * N, M, cap) && sparse_p1c_smem_bytes(cap) <= 227 * 1024)
         return compact_products(h, N, mode_lo, M, kind, cap, d_nb, d_count, d_self, tol, d_m, d_phi, d_k3, s, hook,
                                 packed);
     if (!packed)

@@ -23,10 +23,10 @@ namespace {
 constexpr int PC = 32;  // modes per CTA
 constexpr int PB = 4;   // modes per shared-memory column block
 constexpr int CJ = 8;   // rows per 16-byte store of a BF16 plane
-constexpr int P1T_MODES = 64;     // compact form: modes per CTA (one per thread of a warp pair)
-constexpr int P1T_THREADS = 256;  // compact form: 8 warps
-constexpr int P1T_J = 16;         // compact form: rows j' per chunk (one 32-byte sector per BF16 plane)
-constexpr int P1T_LD = P1T_MODES + 1;  // compact form: row stride of the staged φ rows (odd: no bank conflicts)
+constexpr int P1M_MODES = 64;     // compact form: modes per CTA (two per thread of a warp)
+constexpr int P1M_THREADS = 256;  // compact form: 8 warps
+constexpr int P1M_J = 16;         // compact form: φK rows per store (one 32-byte sector per BF16 plane)
+constexpr int P1M_LD = P1M_MODES + 2;  // compact form: row stride of the staged φ rows (8-byte mode pairs)
 
 struct SparseP1Args {
     int N, n, cap, M, mode_lo;
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(256) sparse_p1_kernel(SparseP1Args a) {
 // Compact first product.  U1[j,k,p] vanishes unless j ∈ nbr(atom(k)), so the
 // compact form keeps, for every column k = 3K + kc and mode p, only the rows
 // of K's neighbourhood in slot order:
-//     U1c[j' + Kc·(p + Mp·k)],  j' = 3·slot + jc < 3·|nbr(K)|, zero up to Kc,
+//     U1c[p + Mp·(j' + Kc·k)],  j' = 3·slot + jc < 3·|nbr(K)|, zero up to Kc,
 // and, as the second product's per-atom operand, the same rows of φ:
 //     φK[j' + Kc·(q + M·K)] = φ[3·nbr(K)[slot] + jc, q].
 // The second product is then a grouped GEMM over the atoms with Kc (about
@@ -266,7 +266,7 @@ __device__ __forceinline__ void st_v8(void* p, const uint32_t (&v)[8]) {
 // Split 16 consecutive values into the hi/lo planes at element offset `off`
 // (a multiple of 16): 32 bytes per BF16 plane, 64 per TF32 plane.
 template <int KIND>
-__device__ __forceinline__ void store_chunk16(void* hi, void* lo, int64_t off, const float (&v)[P1T_J]) {
+__device__ __forceinline__ void store_chunk16(void* hi, void* lo, int64_t off, const float (&v)[P1M_J]) {
     if constexpr (KIND == 1) {
         uint32_t h[8], l[8];
 #pragma unroll
@@ -296,186 +296,165 @@ __device__ __forceinline__ void store_chunk16(void* hi, void* lo, int64_t off, c
     }
 }
 
-// One chunk of 16 rows j' = j0..j0+15 (j0 % 16 == 0, R = j0 % 3) of the three
-// columns k = 3K + kc for this thread's mode: x[s][t] are the staged φ values
-// of the slots j0/3 .. j0/3 + 5 (DOF t), y[t] those of atom K itself.  Every
-// entry is c0·x0 then five fused multiply-adds in the order of the reference
-// contraction's terms (the ASR self rows come from `self`).
-template <int KIND, int R>
-__device__ __forceinline__ void p1t_chunk(const float* __restrict__ cp, int L, int j0, int n3, int ss,
-                                          const float (&x)[6][3], const float (&y)[3],
-                                          const float* __restrict__ selfp, void* hi, void* lo, int64_t off,
-                                          int64_t kc_stride) {
-    // operands of the row pairs (j0 + 2i, j0 + 2i + 1): slot of row j0 + jj is (R + jj) / 3
-    float2 xs[3][8];
-#pragma unroll
-    for (int t = 0; t < 3; ++t)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) xs[t][i] = make_float2(x[(R + 2 * i) / 3][t], x[(R + 2 * i + 1) / 3][t]);
-    const float2 y0 = make_float2(y[0], y[0]), y1 = make_float2(y[1], y[1]), y2 = make_float2(y[2], y[2]);
-    const int sl0 = j0 / 3;
-    const bool has_self = 3 * ss + 2 >= j0 && 3 * ss <= j0 + P1T_J - 1;
-#pragma unroll
-    for (int kc = 0; kc < 3; ++kc) {
-        float2 acc[8];
-        const float* c = cp + (int64_t)(kc * 6) * L + j0;
-#pragma unroll
-        for (int t = 0; t < 6; ++t) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float4 cq = *reinterpret_cast<const float4*>(c + t * L + 4 * q);
-                const float2 ca = make_float2(cq.x, cq.y), cb = make_float2(cq.z, cq.w);
-                const float2 za = t < 3 ? xs[t < 3 ? t : 0][2 * q] : t == 3 ? y0 : t == 4 ? y1 : y2;
-                const float2 zb = t < 3 ? xs[t < 3 ? t : 0][2 * q + 1] : t == 3 ? y0 : t == 4 ? y1 : y2;
-                if (t == 0) {
-                    acc[2 * q] = mul2(ca, za);
-                    acc[2 * q + 1] = mul2(cb, zb);
-                } else {
-                    acc[2 * q] = fma2(ca, za, acc[2 * q]);
-                    acc[2 * q + 1] = fma2(cb, zb, acc[2 * q + 1]);
-                }
-            }
-        }
-        float v[P1T_J];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            v[2 * i] = acc[i].x;
-            v[2 * i + 1] = acc[i].y;
-        }
-        // the self slot's rows: the ASR sums (its pair coefficients are zero)
-        if (has_self) {
-#pragma unroll
-            for (int jj = 0; jj < P1T_J; ++jj)
-                if ((R + jj) / 3 + sl0 == ss) v[jj] = selfp[(kc * 3 + (R + jj) % 3) * P1T_MODES];
-        }
-        // rows past the neighbourhood are exact zeros
-        if (j0 + P1T_J > n3) {
-#pragma unroll
-            for (int jj = 0; jj < P1T_J; ++jj)
-                if (j0 + jj >= n3) v[jj] = 0.f;
-        }
-        store_chunk16<KIND>(hi, lo, off + kc * kc_stride, v);
+// Split a pair of values (two consecutive modes) into the hi/lo planes at
+// element offset `off` (even): 4 bytes per BF16 plane, 8 per TF32 plane.
+template <int KIND>
+__device__ __forceinline__ void store_mode_pair(void* hi, void* lo, int64_t off, float2 v) {
+    if constexpr (KIND == 1) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(v.x - __low2float(h), v.y - __high2float(h));
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(hi) + off) = h;
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(lo) + off) = l;
+    } else {
+        uint32_t b0, b1;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b0) : "f"(v.x));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b1) : "f"(v.y));
+        const float h0 = __uint_as_float(b0), h1 = __uint_as_float(b1);
+        *reinterpret_cast<float2*>(static_cast<float*>(hi) + off) = make_float2(h0, h1);
+        *reinterpret_cast<float2*>(static_cast<float*>(lo) + off) = make_float2(v.x - h0, v.y - h1);
     }
 }
 
-// One CTA per (atom K, P1T_MODES modes), one thread per mode: a thread walks
-// the rows j' of K's neighbourhood in chunks of 16 for all three columns
-// 3K + kc at once, with the staged φ values of its mode in registers and the
-// coefficient rows read as shared-memory broadcasts, and stores each chunk of
-// 16 rows as one 32-byte sector per BF16 plane (its mode's rows are contiguous
-// in U1c).
-// Warps 0-5 first form the ASR self sums of column kc = warp / 2 (in the
-// reference's term order), while warps 6-7 write the φK rows; after one
-// barrier the chunks go round-robin to the four warp pairs.  Rows p ≥ M (up
-// to Mp) are written as zeros.
+// One CTA per (atom K, P1M_MODES modes); a thread holds two consecutive
+// modes, so every store of a warp is 128 contiguous bytes of one BF16 plane:
+// U1c is written mode-fastest, U1c[p + Mp·(j' + Kc·k)], and read by the second
+// product as an MN-major A operand.  After staging (the φ rows of K's
+// neighbourhood, and the pair coefficients rearranged per slot with every
+// value doubled for the packed f32x2 arithmetic), warps 0-2 form the ASR self
+// sums of column kc = warp (in the reference's term order) and warps 3-7 write
+// the φK rows; then the slots go round-robin to the 8 warps, a warp computing
+// the 9 rows (kc, jc) of its slot for all 64 modes.  Every entry is c0·x0 then
+// five fused multiply-adds, as in the reference contraction's term order.
+// Rows j' from 3·|nbr(K)| up to Kc, and modes p ≥ M (up to Mp), are zeros.
 template <int KIND>
-__global__ void __launch_bounds__(P1T_THREADS, 2) sparse_p1t_kernel(SparseP1cArgs a) {
+__global__ void __launch_bounds__(P1M_THREADS, 2) sparse_p1m_kernel(SparseP1cArgs a) {
     extern __shared__ float sm[];
-    const int K = blockIdx.y, p0 = blockIdx.x * P1T_MODES;
+    const int K = blockIdx.y, p0 = blockIdx.x * P1M_MODES;
     const int L = 3 * a.cap;
     const int cnt = a.count[K], ss = a.self_slot[K];
     if (cnt > a.cap) return;  // reported by the coefficient kernel; the output is invalid
     const int n3 = 3 * cnt;
-    float* phis = sm;                          // [L][P1T_LD], mode fastest
-    float* cp = phis + L * P1T_LD;             // pair part [kc][t][L], then self part [kc][jc][L]
-    float* cs = cp + 18 * L;
-    float* selfres = cp + 27 * L;              // [kc][jc][P1T_MODES]
+    float* phis = sm;                              // [L][P1M_LD], mode fastest
+    float* cdup = phis + L * P1M_LD;               // [slot][kc][jc][t][2]: 108 floats per slot
+    float* cs = cdup + 108 * a.cap;                // self part [kc][jc][L]
+    float* selfres = cs + 9 * L;                   // [kc][jc][P1M_MODES]
     const int* nbK = a.nb + (int64_t)K * a.N;
+    const float* coefK = a.coef + (int64_t)K * 27 * L;
     for (int il = threadIdx.x; il < L; il += blockDim.x) {
         const int sl = il / 3;
         const bool live = sl < cnt;
         const float* src = a.phi + (live ? (int64_t)(3 * nbK[sl] + il % 3) + (int64_t)a.n * (a.mode_lo + p0) : 0);
 #pragma unroll 8
-        for (int pp = 0; pp < P1T_MODES; ++pp)
-            phis[il * P1T_LD + pp] = (live && p0 + pp < a.M) ? src[(int64_t)a.n * pp] : 0.f;
+        for (int pp = 0; pp < P1M_MODES; ++pp)
+            phis[il * P1M_LD + pp] = (live && p0 + pp < a.M) ? src[(int64_t)a.n * pp] : 0.f;
+    }
+    for (int r = 0; r < 18; ++r) {                 // pair part: row r = kc·6 + t of the table
+        const int kc = r / 6, t = r - 6 * kc;
+        for (int j = threadIdx.x; j < L; j += blockDim.x) {
+            const int sl = j / 3, jc = j - 3 * sl;
+            const float c = coefK[r * L + j];
+            *reinterpret_cast<float2*>(cdup + ((sl * 9 + kc * 3 + jc) * 6 + t) * 2) = make_float2(c, c);
+        }
     }
     {
-        const float4* cg = reinterpret_cast<const float4*>(a.coef + (int64_t)K * 27 * L);
-        float4* c4 = reinterpret_cast<float4*>(cp);
-        for (int e = threadIdx.x; e < 27 * L / 4; e += blockDim.x) c4[e] = cg[e];
+        const float4* cg = reinterpret_cast<const float4*>(coefK + 18 * L);
+        float4* c4 = reinterpret_cast<float4*>(cs);
+        for (int e = threadIdx.x; e < 9 * L / 4; e += blockDim.x) c4[e] = cg[e];
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p = (warp & 1) * 32 + lane;      // this thread's mode (p0 + p)
-    const int npk = a.Kc / P1T_J;              // chunks of 16 rows
-    if (warp < 6) {
+    const int pm = 2 * lane;                       // this thread's modes p0 + pm, p0 + pm + 1
+    if (warp < 3) {
         // self sums of column kc: Σ_il cs[kc][jc][il] · φ[il, p], il ascending
-        const int kc = warp >> 1;
+        const int kc = warp;
         const float* c0 = cs + (kc * 3) * L;
         const float* c1 = c0 + L;
         const float* c2 = c1 + L;
-        float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+        float2 s0 = make_float2(0.f, 0.f), s1 = s0, s2 = s0;
         int il = 0;
         for (; il + 4 <= n3; il += 4) {
             const float4 a0 = *reinterpret_cast<const float4*>(c0 + il);
             const float4 a1 = *reinterpret_cast<const float4*>(c1 + il);
             const float4 a2 = *reinterpret_cast<const float4*>(c2 + il);
-            const float* ph = phis + il * P1T_LD + p;
-            const float f0 = ph[0], f1 = ph[P1T_LD], f2 = ph[2 * P1T_LD], f3 = ph[3 * P1T_LD];
-            s0 = fmaf(a0.x, f0, s0);
-            s1 = fmaf(a1.x, f0, s1);
-            s2 = fmaf(a2.x, f0, s2);
-            s0 = fmaf(a0.y, f1, s0);
-            s1 = fmaf(a1.y, f1, s1);
-            s2 = fmaf(a2.y, f1, s2);
-            s0 = fmaf(a0.z, f2, s0);
-            s1 = fmaf(a1.z, f2, s1);
-            s2 = fmaf(a2.z, f2, s2);
-            s0 = fmaf(a0.w, f3, s0);
-            s1 = fmaf(a1.w, f3, s1);
-            s2 = fmaf(a2.w, f3, s2);
+            const float* ph = phis + il * P1M_LD + pm;
+            const float2 f0 = *reinterpret_cast<const float2*>(ph);
+            const float2 f1 = *reinterpret_cast<const float2*>(ph + P1M_LD);
+            const float2 f2 = *reinterpret_cast<const float2*>(ph + 2 * P1M_LD);
+            const float2 f3 = *reinterpret_cast<const float2*>(ph + 3 * P1M_LD);
+            s0 = fma2(make_float2(a0.x, a0.x), f0, s0);
+            s1 = fma2(make_float2(a1.x, a1.x), f0, s1);
+            s2 = fma2(make_float2(a2.x, a2.x), f0, s2);
+            s0 = fma2(make_float2(a0.y, a0.y), f1, s0);
+            s1 = fma2(make_float2(a1.y, a1.y), f1, s1);
+            s2 = fma2(make_float2(a2.y, a2.y), f1, s2);
+            s0 = fma2(make_float2(a0.z, a0.z), f2, s0);
+            s1 = fma2(make_float2(a1.z, a1.z), f2, s1);
+            s2 = fma2(make_float2(a2.z, a2.z), f2, s2);
+            s0 = fma2(make_float2(a0.w, a0.w), f3, s0);
+            s1 = fma2(make_float2(a1.w, a1.w), f3, s1);
+            s2 = fma2(make_float2(a2.w, a2.w), f3, s2);
         }
         for (; il < n3; ++il) {
-            const float ph = phis[il * P1T_LD + p];
-            s0 = fmaf(c0[il], ph, s0);
-            s1 = fmaf(c1[il], ph, s1);
-            s2 = fmaf(c2[il], ph, s2);
+            const float2 ph = *reinterpret_cast<const float2*>(phis + il * P1M_LD + pm);
+            s0 = fma2(make_float2(c0[il], c0[il]), ph, s0);
+            s1 = fma2(make_float2(c1[il], c1[il]), ph, s1);
+            s2 = fma2(make_float2(c2[il], c2[il]), ph, s2);
         }
-        selfres[(kc * 3 + 0) * P1T_MODES + p] = s0;
-        selfres[(kc * 3 + 1) * P1T_MODES + p] = s1;
-        selfres[(kc * 3 + 2) * P1T_MODES + p] = s2;
-    } else if (p0 + p < a.M) {
-        // φK rows of this mode: φK[j' + Kc·(q + M·K)], zero past the neighbourhood
-        const int64_t base = (int64_t)a.Kc * ((p0 + p) + (int64_t)a.M * K);
-        for (int ck = 0; ck < npk; ++ck) {
-            float v[P1T_J];
+        *reinterpret_cast<float2*>(selfres + (kc * 3 + 0) * P1M_MODES + pm) = s0;
+        *reinterpret_cast<float2*>(selfres + (kc * 3 + 1) * P1M_MODES + pm) = s1;
+        *reinterpret_cast<float2*>(selfres + (kc * 3 + 2) * P1M_MODES + pm) = s2;
+    } else {
+        // φK rows: φK[j' + Kc·(q + M·K)], zero past the neighbourhood, 16 rows
+        // of a mode per task (one 32-byte sector per BF16 plane)
+        const int npk = a.Kc / P1M_J;
+        for (int task = threadIdx.x - 96; task < P1M_MODES * npk; task += P1M_THREADS - 96) {
+            const int q = task % P1M_MODES, ck = task / P1M_MODES;
+            if (p0 + q >= a.M) continue;
+            float v[P1M_J];
 #pragma unroll
-            for (int jj = 0; jj < P1T_J; ++jj) {
-                const int j = ck * P1T_J + jj;
-                v[jj] = j < n3 ? phis[j * P1T_LD + p] : 0.f;
+            for (int jj = 0; jj < P1M_J; ++jj) {
+                const int j = ck * P1M_J + jj;
+                v[jj] = j < n3 ? phis[j * P1M_LD + q] : 0.f;
             }
-            store_chunk16<KIND>(a.pk_hi, a.pk_lo, base + ck * P1T_J, v);
+            store_chunk16<KIND>(a.pk_hi, a.pk_lo, (int64_t)a.Kc * ((p0 + q) + (int64_t)a.M * K) + ck * P1M_J, v);
         }
     }
     __syncthreads();
-    float y[3];
+    float2 y[3];
 #pragma unroll
-    for (int t = 0; t < 3; ++t) y[t] = phis[(3 * ss + t) * P1T_LD + p];
-    const int64_t off0 = (int64_t)a.Kc * ((p0 + p) + (int64_t)a.Mp * (3 * K));
-    const int64_t kc_stride = (int64_t)a.Kc * a.Mp;
-    const float* selfp = selfres + p;
-    for (int ck = warp >> 1; ck < npk; ck += P1T_THREADS / 64) {
-        const int j0 = ck * P1T_J;
-        const int sl0 = j0 / 3;
-        float x[6][3];
+    for (int t = 0; t < 3; ++t) y[t] = *reinterpret_cast<const float2*>(phis + (3 * ss + t) * P1M_LD + pm);
+    // U1c[p + Mp·(j' + Kc·(3K + kc))]
+    const int64_t colK = (int64_t)a.Kc * (3 * K);
+    const int64_t pbase = p0 + pm;
+    for (int sl = warp; sl < cnt; sl += P1M_THREADS / 32) {
+        float2 x[3];
 #pragma unroll
-        for (int s = 0; s < 6; ++s)
+        for (int t = 0; t < 3; ++t) x[t] = *reinterpret_cast<const float2*>(phis + (3 * sl + t) * P1M_LD + pm);
+        const float4* cq = reinterpret_cast<const float4*>(cdup + sl * 108);
+        const bool self = sl == ss;
 #pragma unroll
-            for (int t = 0; t < 3; ++t) {
-                const int row = 3 * (sl0 + s) + t;
-                x[s][t] = row < L ? phis[row * P1T_LD + p] : 0.f;
+        for (int kc = 0; kc < 3; ++kc)
+#pragma unroll
+            for (int jc = 0; jc < 3; ++jc) {
+                const float4 q0 = cq[(kc * 3 + jc) * 3], q1 = cq[(kc * 3 + jc) * 3 + 1],
+                             q2 = cq[(kc * 3 + jc) * 3 + 2];
+                float2 v = mul2(make_float2(q0.x, q0.y), x[0]);
+                v = fma2(make_float2(q0.z, q0.w), x[1], v);
+                v = fma2(make_float2(q1.x, q1.y), x[2], v);
+                v = fma2(make_float2(q1.z, q1.w), y[0], v);
+                v = fma2(make_float2(q2.x, q2.y), y[1], v);
+                v = fma2(make_float2(q2.z, q2.w), y[2], v);
+                if (self) v = *reinterpret_cast<const float2*>(selfres + (kc * 3 + jc) * P1M_MODES + pm);
+                store_mode_pair<KIND>(a.u1_hi, a.u1_lo,
+                                      pbase + (int64_t)a.Mp * ((3 * sl + jc) + colK + (int64_t)a.Kc * kc), v);
             }
-        switch (j0 % 3) {
-            case 0:
-                p1t_chunk<KIND, 0>(cp, L, j0, n3, ss, x, y, selfp, a.u1_hi, a.u1_lo, off0 + j0, kc_stride);
-                break;
-            case 1:
-                p1t_chunk<KIND, 1>(cp, L, j0, n3, ss, x, y, selfp, a.u1_hi, a.u1_lo, off0 + j0, kc_stride);
-                break;
-            default:
-                p1t_chunk<KIND, 2>(cp, L, j0, n3, ss, x, y, selfp, a.u1_hi, a.u1_lo, off0 + j0, kc_stride);
-                break;
-        }
+    }
+    // rows past the neighbourhood
+    const int nz = a.Kc - n3;
+    for (int e = warp; e < 3 * nz; e += P1M_THREADS / 32) {
+        const int kc = e / nz, j = n3 + (e - kc * nz);
+        store_mode_pair<KIND>(a.u1_hi, a.u1_lo, pbase + (int64_t)a.Mp * (j + colK + (int64_t)a.Kc * kc),
+                              make_float2(0.f, 0.f));
     }
 }
 
@@ -525,7 +504,7 @@ namespace fcb {
 
 size_t sparse_p1c_smem_bytes(int cap) {
     const size_t L = 3 * (size_t)cap;
-    return sizeof(float) * (L * P1T_LD + 27 * L + 9 * P1T_MODES);
+    return sizeof(float) * (L * P1M_LD + 108 * (size_t)cap + 9 * L + 9 * P1M_MODES);
 }
 
 int sparse_p1c_launch(int kind, int64_t N, int cap, const int* d_nb, const int* d_count, const int* d_self,
@@ -549,13 +528,13 @@ int sparse_p1c_launch(int kind, int64_t N, int cap, const int* d_nb, const int* 
     a.pk_hi = pk_hi;
     a.pk_lo = pk_lo;
     const size_t smem = sparse_p1c_smem_bytes(cap);
-    const dim3 grid((unsigned)(Mp / P1T_MODES), (unsigned)N);
+    const dim3 grid((unsigned)(Mp / P1M_MODES), (unsigned)N);
     if (kind == 1) {
-        FCB_CUDA(cudaFuncSetAttribute(sparse_p1t_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        sparse_p1t_kernel<1><<<grid, P1T_THREADS, smem, s>>>(a);
+        FCB_CUDA(cudaFuncSetAttribute(sparse_p1m_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sparse_p1m_kernel<1><<<grid, P1M_THREADS, smem, s>>>(a);
     } else {
-        FCB_CUDA(cudaFuncSetAttribute(sparse_p1t_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        sparse_p1t_kernel<2><<<grid, P1T_THREADS, smem, s>>>(a);
+        FCB_CUDA(cudaFuncSetAttribute(sparse_p1m_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sparse_p1m_kernel<2><<<grid, P1M_THREADS, smem, s>>>(a);
     }
     FCB_CUDA(cudaGetLastError());
     return FCB_OK;
