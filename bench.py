@@ -703,7 +703,7 @@ def main():
         else:    # hi + lo BF16 planes of the dense-layout U1
             u1_bytes = 4.0 * n ** 3
         p1_ms = float(phases[3])
-        sparse_p1 = {"kernel": "sparse_p1c_kernel (compact, CUDA cores, FP32)" if cs else
+        sparse_p1 = {"kernel": "sparse_p1m_kernel (compact, CUDA cores, FP32, U1c mode-fastest)" if cs else
                      "sparse_p1_kernel (CUDA cores, FP32)", "ms": round(p1_ms, 4),
                      "bytes_written": u1_bytes, "achieved_gbs": round(u1_bytes / (p1_ms * 1e-3) / 1e9, 1),
                      "frac_of_hbm": round(u1_bytes / (p1_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)}
