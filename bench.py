@@ -46,7 +46,7 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustain
 # grouped second product 0.759e9 + 1.157e9, its MN-major third product
 # 1.541e9 + 1.764e9, the FP64 writer 0.005e9 + 3.561e9; the dense-layout
 # symmetric product (taken where the compact form does not pay) 3.770e9.
-NCU_TRAFFIC = {"mode_product_tc2_p2": 1.916e9, "mode_product_tc2_p3": 3.305e9, "mode_product_tc2_sym": 3.770e9,
+NCU_TRAFFIC = {"mode_product_tc2_p2": 1.914e9, "mode_product_tc2_p3": 3.138e9, "mode_product_tc2_sym": 3.770e9,
                "ifc3_dense_psi64": 3.566e9}
 
 
