@@ -701,7 +701,9 @@ int sparse_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, in
 // product (U1c and the per-atom φ rows), the grouped second product
 // (U2[p + Mp·k + Mp·n·q], one B per atom, symmetric in (p, q)) and the third
 // product reading U2 MN-major (phase marks 3..5; the caller splits φ before and
-// marks 6 after).  hook() is called before the third product.
+// marks 6 after).  hook() is called before the first product: the FP64 Ψ
+// writer it starts shares the SMs with the first product (CUDA cores, light
+// on DRAM) and then with the two tensor-core products.
 template <class Hook>
 int compact_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, int kind, int cap, const int* d_nb,
                      const int* d_count, const int* d_self, double tol, const double* d_m, const float* d_phi,
@@ -710,6 +712,7 @@ int compact_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, i
     const int64_t np = pad_for(kind, n);
     const int64_t Mp = compact_Mp(M), Kc = compact_Kc(cap);
     const size_t esz = esz_of(kind);
+    FCB_TRY(hook());
     FCB_TRY(h->sp_coef.ensure(sizeof(float) * (size_t)N * 27 * 3 * cap));
     FCB_TRY(lj_sparse_coefs(h, N, tol, d_m, d_nb, d_count, d_self, cap, h->sp_coef.as<float>(), s));
     phase_mark(h, s, 3);
@@ -732,7 +735,6 @@ int compact_products(fcb200_context* h, int64_t N, int64_t mode_lo, int64_t M, i
     FCB_TRY(mode_product_tc(h, kind, h->u1_hi.p, h->u1_lo.p, h->phik_hi.p, h->phik_lo.p, h->u2_hi.p, h->u2_lo.p, kind,
                             p2, s));
     phase_mark(h, s, 5);
-    FCB_TRY(hook());
     const size_t poff = esz * np * mode_lo;
     ModeProduct p3{Mp * M, n, M, Mp, np, Mp, M, M * M};
     p3.sym_full = true;  // row tiles with p / 256 <= q / 256, K3 stored by its full symmetry
@@ -767,10 +769,11 @@ int sparse_snapshot_products(fcb200_context* h, int64_t N, int64_t mode_lo, int6
 // Needs the largest neighbour count on the host to size the coefficient
 // tables, so it synchronises the stream once (after the neighbour lists; the
 // φ split is already queued behind them), unless the handle has a fixed
-// neighbour capacity (then an overflow is reported by the status word).  The FP64 Ψ writer (HBM-bound) runs
-// on the aux stream beside the tensor-core bound products (the third one in
-// the compact form, the second and third otherwise), with two blocks per SM
-// so that both kernels stay resident on every SM; the caller's stream waits
+// neighbour capacity (then an overflow is reported by the status word).  The
+// FP64 Ψ writer (HBM-bound) runs on the aux stream beside the products (from
+// the first one on in the compact form, the second and third otherwise), with
+// two blocks per SM so that they stay resident beside the pair kernel's CTA
+// (one beside the first product's two); the caller's stream waits
 // for it before the end (with phase timing on it runs alone instead, before
 // the sparse products).  Sets *used = false, having done nothing visible, when
 // the neighbourhoods are so large that the sparse form does not pay; the

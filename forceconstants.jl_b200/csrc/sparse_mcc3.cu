@@ -326,8 +326,11 @@ __device__ __forceinline__ void store_mode_pair(void* hi, void* lo, int64_t off,
 // the 9 rows (kc, jc) of its slot for all 64 modes.  Every entry is c0·x0 then
 // five fused multiply-adds, as in the reference contraction's term order.
 // Rows j' from 3·|nbr(K)| up to Kc, and modes p ≥ M (up to Mp), are zeros.
+// Held to 96 registers: two CTAs (2 × 256 × 96) leave room on every SM for
+// one 256-thread block of the FP64 Ψ writer (64 registers), which the
+// snapshot path starts beside this kernel on a second stream.
 template <int KIND>
-__global__ void __launch_bounds__(P1M_THREADS, 2) sparse_p1m_kernel(SparseP1cArgs a) {
+__global__ void __maxnreg__(96) sparse_p1m_kernel(SparseP1cArgs a) {
     extern __shared__ float sm[];
     const int K = blockIdx.y, p0 = blockIdx.x * P1M_MODES;
     const int L = 3 * a.cap;
