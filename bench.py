@@ -132,8 +132,50 @@ class Clocks:
         self.idx = gpu_index
         self.proc = None
         self.path = os.path.join(out_dir, f"clocks_bench_{os.getpid()}.csv")
+        self.nvml = None
+        self.samples = []
+
+    def _nvml_handle(self):
+        """NVML handle of the CUDA device `idx` (matched by PCI bus id, so that a
+        CUDA_VISIBLE_DEVICES mapping does not pick another GPU)."""
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            pr = torch.cuda.get_device_properties(self.idx)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+
+    def _poll(self):
+        nv, h = self.nvml
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self.halt.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((sm, [k for k, b in bits.items() if r & b]))
+            except Exception:
+                return
+            time.sleep(0.002)
 
     def start(self):
+        """nvidia-smi writes its CSV record (100 ms period) and an NVML thread
+        samples the SM clock and the throttle reasons every 2 ms, so that a
+        timed region of a few tens of milliseconds still holds samples."""
+        import threading
+        try:
+            self.nvml = self._nvml_handle()
+            self.smax = self.nvml[0].nvmlDeviceGetMaxClockInfo(self.nvml[1], self.nvml[0].NVML_CLOCK_SM)
+            self.halt = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.nvml = None
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
@@ -144,8 +186,16 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        nvml = None
+        if self.nvml is not None:
+            self.halt.set()
+            self.thread.join(timeout=5)
+            if self.samples:
+                nvml = {"sm_mhz": statistics.median(x[0] for x in self.samples), "sm_max_mhz": float(self.smax),
+                        "reasons": sorted({r for x in self.samples for r in x[1]}), "samples": len(self.samples),
+                        "source": "NVML, 2 ms period, timed region only"}
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return nvml or {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.25)
         self.proc.terminate()
         try:
@@ -167,8 +217,12 @@ class Clocks:
             for nm, v in zip(names, parts[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        smi = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+               "reasons": sorted(reasons), "samples": len(sm)}
+        if nvml is None:
+            return smi
+        nvml["nvidia_smi"] = smi  # 100 ms record, including the 0.25 s after the timed region
+        return nvml
 
 
 def build_workload(fcb, device):
