@@ -5,7 +5,8 @@
 //
 // 128×128 output tile per 256-thread CTA, 16-deep K slices double-buffered in
 // shared memory (stored transposed so the inner loop reads broadcast-friendly
-// float4 rows), an 8×8 register micro-tile per thread.  Thread (tr, tp) owns
+// float4 rows), an 8×8 register micro-tile per thread, accumulated as column
+// pairs by packed f32x2 FMAs (half the FMA instructions).  Thread (tr, tp) owns
 // rows {4tr..4tr+3, 64+4tr..} and columns {4tp.., 64+4tp..}; lanes of a warp
 // vary along r, the contiguous output index, so each float4 store of a warp is
 // a 256-byte contiguous segment.
@@ -16,8 +17,21 @@ namespace {
 
 constexpr int TM = 128, TN = 128, TK = 16, PAD = 4;
 
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<const uint64_t*>(&a)), "l"(*reinterpret_cast<const uint64_t*>(&b)),
+          "l"(*reinterpret_cast<const uint64_t*>(&c)));
+    return *reinterpret_cast<const float2*>(&d);
+}
+
+__device__ __forceinline__ float accv(const float2 (&acc)[8][4], int i, int j) {
+    return (j & 1) ? acc[i][j >> 1].y : acc[i][j >> 1].x;
+}
+
 template <bool VEC>
-__global__ void __launch_bounds__(256) mode_product_f32_kernel(const float* __restrict__ A,
+__global__ void __launch_bounds__(256, 2) mode_product_f32_kernel(const float* __restrict__ A,
                                                                const float* __restrict__ B,
                                                                float* __restrict__ D, ModeProduct mp) {
     __shared__ __align__(16) float As[2][TK][TM + PAD];
@@ -67,11 +81,13 @@ __global__ void __launch_bounds__(256) mode_product_f32_kernel(const float* __re
         }
     };
 
-    float acc[8][8];
+    // acc[i][jp] holds columns (2jp, 2jp+1) of row i: packed f32x2 FMAs, each
+    // half rounded as fmaf rounds it
+    float2 acc[8][4];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+        for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.f, 0.f);
 
     const int64_t nk = (mp.K + TK - 1) / TK;
     fetch(0);
@@ -87,11 +103,14 @@ __global__ void __launch_bounds__(256) mode_product_f32_kernel(const float* __re
             const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][k][4 * tp]);
             const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][k][64 + 4 * tp]);
             const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            const float2 b[4] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w), make_float2(b1.x, b1.y),
+                                 make_float2(b1.z, b1.w)};
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
+            for (int i = 0; i < 8; ++i) {
+                const float2 ai = make_float2(a[i], a[i]);
 #pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) acc[i][j] = ffma2(ai, b[j], acc[i][j]);
+            }
         }
         if (kt + 1 < nk) stash(buf ^ 1);
         __syncthreads();
@@ -106,13 +125,13 @@ __global__ void __launch_bounds__(256) mode_product_f32_kernel(const float* __re
             const int64_t rb0 = r0 + 64 * h + 4 * tr;
             if (VEC && rb0 + 3 < mp.R) {
                 const int64_t off = (rb0 % mp.F) + mp.F_pad * (rb0 / mp.F) + mp.ldd * p;
-                *reinterpret_cast<float4*>(D + off) =
-                    make_float4(acc[4 * h + 0][j], acc[4 * h + 1][j], acc[4 * h + 2][j], acc[4 * h + 3][j]);
+                *reinterpret_cast<float4*>(D + off) = make_float4(accv(acc, 4 * h + 0, j), accv(acc, 4 * h + 1, j),
+                                                                  accv(acc, 4 * h + 2, j), accv(acc, 4 * h + 3, j));
             } else {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int64_t r = rb0 + u;
-                    if (r < mp.R) D[(r % mp.F) + mp.F_pad * (r / mp.F) + mp.ldd * p] = acc[4 * h + u][j];
+                    if (r < mp.R) D[(r % mp.F) + mp.F_pad * (r / mp.F) + mp.ldd * p] = accv(acc, 4 * h + u, j);
                 }
             }
         }
