@@ -88,31 +88,47 @@ __global__ void sw_neighbor_kernel(const double* __restrict__ pos, const double*
     npair[i] = up;
 }
 
-// Exclusive scan of `len` ints by one CTA (out has len + 1 entries).
+// Exclusive scan of `len` ints by one CTA (out has len + 1 entries): tiles of
+// 4 consecutive ints per thread, scanned across the block with warp shuffles,
+// a running carry between tiles.
 __global__ void scan_kernel(const int* __restrict__ in, int64_t len, int* __restrict__ out) {
-    __shared__ int part[1024];
-    const int t = threadIdx.x, T = blockDim.x;
-    const int64_t chunk = (len + T - 1) / T;
-    const int64_t b = t * chunk, e = b + chunk < len ? b + chunk : len;
-    int s = 0;
-    for (int64_t i = b; i < e; ++i) s += in[i];
-    part[t] = s;
-    __syncthreads();
-    if (t == 0) {
-        int acc = 0;
-        for (int i = 0; i < T; ++i) {
-            const int v = part[i];
-            part[i] = acc;
-            acc += v;
+    __shared__ int wsum[32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
+    int carry = 0;
+    for (int64_t base = 0; base < len; base += 4 * (int64_t)blockDim.x) {
+        const int64_t i0 = base + 4 * (int64_t)t;
+        int v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = i0 + u < len ? in[i0 + u] : 0;
+        const int tsum = v[0] + v[1] + v[2] + v[3];
+        int x = tsum;  // inclusive scan within the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
         }
-        out[len] = acc;
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int w = lane < nw ? wsum[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            if (lane < nw) wsum[lane] = w;
+        }
+        __syncthreads();
+        int acc = carry + (warp ? wsum[warp - 1] : 0) + x - tsum;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u < len) out[i0 + u] = acc;
+            acc += v[u];
+        }
+        carry += wsum[nw - 1];
+        __syncthreads();  // wsum is rewritten by the next tile
     }
-    __syncthreads();
-    int acc = part[t];
-    for (int64_t i = b; i < e; ++i) {
-        out[i] = acc;
-        acc += in[i];
-    }
+    if (t == 0) out[len] = carry;
 }
 
 __device__ __forceinline__ int find_owner(const int* __restrict__ off, int N, int t) {
@@ -524,20 +540,63 @@ __global__ void bucket_fill_kernel(const Place* __restrict__ pl, int n, int kind
     if (bucket_of(pl[t], kind, N, &key)) items[atomicAdd(&cursor[key], 1)] = t;
 }
 
+// One warp per bucket: every item's rank is the number of items ordered
+// before it by (sort key, placement index) — the placement index breaks ties,
+// so the order does not depend on the order in which bucket_fill's atomics
+// placed the items — and each lane then writes its items to their ranks.
+// Buckets of more than SORT_REG·32 items fall back to an insertion sort by
+// lane 0 with the same order.
+constexpr int SORT_REG = 8;
+
+__device__ __forceinline__ bool key_before(long long ka, int ia, long long kb, int ib) {
+    return ka < kb || (ka == kb && ia < ib);
+}
+
 __global__ void bucket_sort_kernel(const Place* __restrict__ pl, int kind, int nb, const int* __restrict__ off,
                                    int* __restrict__ items) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
-    const int s = off[b], e = off[b + 1];
-    for (int x = s + 1; x < e; ++x) {  // insertion sort: deterministic order
-        const int it = items[x];
-        const long long k = sort_key(pl[it], kind);
-        int y = x - 1;
-        while (y >= s && sort_key(pl[items[y]], kind) > k) {
-            items[y + 1] = items[y];
-            --y;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += warps) {
+        const int s = off[b], e = off[b + 1], k = e - s;
+        if (k <= 1) continue;
+        if (k > SORT_REG * 32) {
+            if (lane == 0) {
+                for (int x = s + 1; x < e; ++x) {
+                    const int it = items[x];
+                    const long long kk = sort_key(pl[it], kind);
+                    int y = x - 1;
+                    while (y >= s && key_before(kk, it, sort_key(pl[items[y]], kind), items[y])) {
+                        items[y + 1] = items[y];
+                        --y;
+                    }
+                    items[y + 1] = it;
+                }
+            }
+            __syncwarp();
+            continue;
         }
-        items[y + 1] = it;
+        long long key[SORT_REG];
+        int item[SORT_REG], rank[SORT_REG];
+#pragma unroll
+        for (int r = 0; r < SORT_REG; ++r) {
+            const int i = lane + 32 * r;
+            item[r] = i < k ? items[s + i] : 0x7fffffff;
+            key[r] = i < k ? sort_key(pl[item[r]], kind) : 0x7fffffffffffffffLL;
+            rank[r] = 0;
+        }
+        for (int r2 = 0; r2 < SORT_REG && 32 * r2 < k; ++r2) {
+            for (int l2 = 0; l2 < 32; ++l2) {
+                const long long kj = __shfl_sync(0xffffffffu, key[r2], l2);
+                const int ij = __shfl_sync(0xffffffffu, item[r2], l2);
+#pragma unroll
+                for (int r = 0; r < SORT_REG; ++r) rank[r] += key_before(kj, ij, key[r], item[r]) ? 1 : 0;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < SORT_REG; ++r)
+            if (lane + 32 * r < k) items[s + rank[r]] = item[r];
+        __syncwarp();
     }
 }
 
@@ -638,7 +697,36 @@ __device__ __forceinline__ void sw_store(const SwDense& g, int64_t col, int e, d
     }
 }
 
-// one warp per column (jj,kk); lanes over the rows
+// Two consecutive rows (r, r+1; n and n_pad even) stored as one vector per
+// output: 16 bytes of FP64, 4 (BF16) or 8 (TF32) bytes per split plane.
+__device__ __forceinline__ void sw_store2(const SwDense& g, int64_t col, int e, double r0, double r1, double w0,
+                                          double w1) {
+    if (g.psi64)
+        *reinterpret_cast<double2*>(g.psi64 + col * g.n + e) =
+            g.psi64_weighted ? make_double2(w0, w1) : make_double2(r0, r1);
+    if (g.psi32) *reinterpret_cast<float2*>(g.psi32 + col * g.n + e) = make_float2((float)w0, (float)w1);
+    const int64_t off = col * g.n_pad + e;
+    if (g.split_kind == 1) {
+        const __nv_bfloat16 h0 = __float2bfloat16_rn((float)w0), h1 = __float2bfloat16_rn((float)w1);
+        const __nv_bfloat16 l0 = __float2bfloat16_rn((float)(w0 - (double)__bfloat162float(h0)));
+        const __nv_bfloat16 l1 = __float2bfloat16_rn((float)(w1 - (double)__bfloat162float(h1)));
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(g.split_hi) + off) = __halves2bfloat162(h0, h1);
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(g.split_lo) + off) = __halves2bfloat162(l0, l1);
+    } else if (g.split_kind == 2) {
+        uint32_t b0, b1;
+        const float f0 = (float)w0, f1 = (float)w1;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b0) : "f"(f0));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b1) : "f"(f1));
+        const float h0 = __uint_as_float(b0), h1 = __uint_as_float(b1);
+        *reinterpret_cast<float2*>(static_cast<float*>(g.split_hi) + off) = make_float2(h0, h1);
+        *reinterpret_cast<float2*>(static_cast<float*>(g.split_lo) + off) =
+            make_float2((float)(w0 - (double)h0), (float)(w1 - (double)h1));
+    }
+}
+
+// one warp per column (jj,kk); lanes over the rows (VEC2: two consecutive
+// rows per lane, so every warp store covers one contiguous segment)
+template <bool VEC2>
 __global__ void __launch_bounds__(256) sw_dense_kernel(SwDense g) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -651,13 +739,25 @@ __global__ void __launch_bounds__(256) sw_dense_kernel(SwDense g) {
         const int ab = K * N + J;
         const bool asr_live = g.asr_off[ab] != g.asr_off[ab + 1];
         const bool live = (s != e) || asr_live;
-        for (int r = lane; r < n; r += 32) {
-            double raw = 0.0, mw = 0.0;
-            if (live) {
-                const int I = r / 3, a = r - 3 * I;
-                raw = sw_finish(g, sw_value(g, I, a, J, b, K, c, s, e), I, J, K, &mw);
+        if constexpr (VEC2) {
+            for (int r = 2 * lane; r < n; r += 64) {
+                double raw0 = 0.0, raw1 = 0.0, mw0 = 0.0, mw1 = 0.0;
+                if (live) {
+                    const int I0 = r / 3, a0 = r - 3 * I0, I1 = (r + 1) / 3, a1 = r + 1 - 3 * I1;
+                    raw0 = sw_finish(g, sw_value(g, I0, a0, J, b, K, c, s, e), I0, J, K, &mw0);
+                    raw1 = sw_finish(g, sw_value(g, I1, a1, J, b, K, c, s, e), I1, J, K, &mw1);
+                }
+                sw_store2(g, col, r, raw0, raw1, mw0, mw1);
             }
-            sw_store(g, col, r, raw, mw);
+        } else {
+            for (int r = lane; r < n; r += 32) {
+                double raw = 0.0, mw = 0.0;
+                if (live) {
+                    const int I = r / 3, a = r - 3 * I;
+                    raw = sw_finish(g, sw_value(g, I, a, J, b, K, c, s, e), I, J, K, &mw);
+                }
+                sw_store(g, col, r, raw, mw);
+            }
         }
     }
 }
@@ -778,7 +878,8 @@ static int sw_bucket(fcb200_context* h, Buf& offb, Buf& itemb, Buf& curb, const 
     scan_kernel<<<1, 1024, 0, s>>>(cnt, nb, offb.as<int>());
     FCB_CUDA(cudaMemcpyAsync(cnt, offb.p, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToDevice, s));
     if (np > 0) bucket_fill_kernel<<<(np + 255) / 256, 256, 0, s>>>(P, np, kind, N, cnt, itemb.as<int>());
-    bucket_sort_kernel<<<(nb + 255) / 256, 256, 0, s>>>(P, kind, nb, offb.as<int>(), itemb.as<int>());
+    bucket_sort_kernel<<<(unsigned)((nb + 7) / 8 < 148 * 16 ? (nb + 7) / 8 : 148 * 16), 256, 0, s>>>(
+        P, kind, nb, offb.as<int>(), itemb.as<int>());
     FCB_CUDA(cudaGetLastError());
     (void)h;
     *off = offb.as<int>();
@@ -845,7 +946,10 @@ int sw_third_order_launch(fcb200_context* h, const double* d_pos, int64_t N, con
     const int64_t cols = (int64_t)g.n * g.n;
     int64_t blocks = (cols + 7) / 8;
     if (blocks > (int64_t)h->sm_count * 8) blocks = (int64_t)h->sm_count * 8;
-    sw_dense_kernel<<<(unsigned)blocks, 256, 0, s>>>(g);
+    if (g.n % 2 == 0 && g.n_pad % 2 == 0)
+        sw_dense_kernel<true><<<(unsigned)blocks, 256, 0, s>>>(g);
+    else
+        sw_dense_kernel<false><<<(unsigned)blocks, 256, 0, s>>>(g);
     FCB_CUDA(cudaGetLastError());
     return FCB_OK;
 }
