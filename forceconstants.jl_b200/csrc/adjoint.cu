@@ -6,7 +6,7 @@
 //     L = Σ_ijk G[i,j,k] Ψ_mw[i,j,k],   G = W ×₁ φᵀ ×₂ φᵀ ×₃ φᵀ,
 // i.e. the three transposed mode products of mcc3 (src/mcc.jl:29-51) applied
 // to W.  G runs on the same mode-product kernels (tensor cores or FP32), or in
-// FP64 on the DFMA mode product (FCB_ADJOINT_FP64).
+// FP64 on the FP64 tensor-core mode product (FCB_ADJOINT_FP64).
 //
 // For the analytical LJ calculator every non-zero Ψ block belongs to one
 // ordered pair (A,B) inside the cutoff: the blocks with two A's and one B hold

@@ -237,7 +237,7 @@ int mode_product_f32(const float* A, const float* B, float* D, const ModeProduct
 // = K3[p + M(q + M s)] for p <= q <= s (mcc3.cu).
 int pack_k3_launch(const float* full, int64_t M, float* packed, cudaStream_t s);
 inline int64_t packed_k3_count(int64_t M) { return M * (M + 1) * (M + 2) / 6; }
-// FP64 (DFMA) mode product and an FP32 → FP64 widening copy (mode_product_f64.cu).
+// FP64 mode product (FP64 tensor cores, mma.sync .f64) and an FP32 → FP64 widening copy (mode_product_f64.cu).
 int mode_product_f64(const double* A, const double* B, double* D, const ModeProduct& mp, cudaStream_t s);
 int widen_f32_to_f64(const float* src, double* dst, int64_t count, cudaStream_t s);
 // Finite-difference IFCs (finite_diff.cu).  kind 0 = LJ, 1 = SW.

@@ -48,7 +48,7 @@ extern "C" {
 #define FCB_MCC3_FP32       0  /* plain FP32 SIMT mode products (FFMA)                     */
 #define FCB_MCC3_BF16X3     1  /* split-BF16 on tcgen05: hi·hi + hi·lo + lo·hi, FP32 acc   */
 #define FCB_MCC3_TF32X3     2  /* split-TF32 on tcgen05: hi·hi + hi·lo + lo·hi, FP32 acc   */
-/* fcb200_mcc3_adjoint_lj only: G = W ×₁φᵀ ×₂φᵀ ×₃φᵀ formed in FP64 (DFMA)    */
+/* fcb200_mcc3_adjoint_lj only: G = W ×₁φᵀ ×₂φᵀ ×₃φᵀ formed in FP64 (DMMA)    */
 #define FCB_ADJOINT_FP64    3
 /* OR into the precision of fcb200_snapshot_lj: run the dense first and second
  * mode products even where the block-sparse form applies.                     */
