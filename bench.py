@@ -148,20 +148,35 @@ class Clocks:
         except Exception:
             return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.idx)
 
-    def _poll(self):
+    def _sample(self):
         nv, h = self.nvml
         bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
                 "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
                 "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
                 "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.samples.append((sm, [k for k, b in bits.items() if r & b]))
+
+    def _poll(self):
         while not self.halt.is_set():
             try:
-                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-                self.samples.append((sm, [k for k, b in bits.items() if r & b]))
+                self._sample()
             except Exception:
                 return
             time.sleep(0.002)
+
+    def wait_for(self, event):
+        """Samples from the calling thread until `event` (recorded after the
+        timed steps) has completed, so that the timed region is sampled even
+        when the background thread gets little time."""
+        while not event.query():
+            if self.nvml is not None:
+                try:
+                    self._sample()
+                except Exception:
+                    pass
+            time.sleep(0.0005)
 
     def start(self):
         """nvidia-smi writes its CSV record (100 ms period) and an NVML thread
@@ -193,7 +208,7 @@ class Clocks:
             if self.samples:
                 nvml = {"sm_mhz": statistics.median(x[0] for x in self.samples), "sm_max_mhz": float(self.smax),
                         "reasons": sorted({r for x in self.samples for r in x[1]}), "samples": len(self.samples),
-                        "source": "NVML, 2 ms period, timed region only"}
+                        "source": "NVML, timed region only (polled while the timed steps run)"}
         if self.proc is None:
             return nvml or {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.25)
@@ -644,6 +659,7 @@ def main():
     for _ in range(args.steps):
         step()
     e1.record(stream)
+    clocks.wait_for(e1)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
