@@ -752,13 +752,20 @@ def main():
         if cs:
             p2_ms = float(phases[4])
             a2 = p2_flops / (p2_ms * 1e-3) / 1e12
+            esz2 = 2 if args.precision == "bf16x3" else 4
+            p2_tiles = 3 * s.n_atoms * (Mp // 256) * ((Mp // 256) + 1) // 2   # upper (p, q) tiles per (atom, kc)
+            p2_bytes = 2.0 * esz2 * (Mp * n * Kc + s.n_atoms * n * Kc + p2_tiles * 256 * 256)
             roof["second_product"] = {
                 "kernel": "mode_product_tc2_kernel, grouped by atom (K = Kc), tiles p/256 <= q/256 of U2 only "
                           "(symmetric in (p, q))", "Mp": Mp, "Kc": Kc, "flops_per_launch": p2_flops,
                 "ms": round(p2_ms, 4),
                 "achieved": round(a2, 2), "frac": round(a2 / pk, 4) if pk else None,
                 "traffic": NCU_TRAFFIC.get("mode_product_tc2_p2") if (args.precision == "bf16x3" and n == 768)
-                else None}
+                else None,
+                # its epilogue's stores bound it: the algorithmic bytes (U1c and φK read, upper U2 tiles
+                # written) against the HBM copy bandwidth
+                "algorithmic_bytes": p2_bytes,
+                "frac_of_hbm": round(p2_bytes / (p2_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)}
     asm_bytes = 8.0 * n ** 3 + (0.0 if split else 4.0 * n ** 3)
     asm_ms = float(phases[1])
     roof_asm = {"bound": "hbm", "achieved": round(asm_bytes / (asm_ms * 1e-3) / 1e9, 1), "peak": peaks["hbm_gbs"],
