@@ -27,6 +27,8 @@ constexpr int P1M_MODES = 64;     // compact form: modes per CTA (two per thread
 constexpr int P1M_THREADS = 256;  // compact form: 8 warps
 constexpr int P1M_J = 16;         // compact form: φK rows per store (one 32-byte sector per BF16 plane)
 constexpr int P1M_LD = P1M_MODES + 2;  // compact form: row stride of the staged φ rows (8-byte mode pairs)
+constexpr int P1M_STAGE = 32;     // compact form: φ loads a thread has in flight while staging
+static_assert(P1M_MODES % P1M_STAGE == 0, "the staging batches cover the CTA's modes");
 
 struct SparseP1Args {
     int N, n, cap, M, mode_lo;
@@ -343,26 +345,51 @@ __global__ void __maxnreg__(96) sparse_p1m_kernel(SparseP1cArgs a) {
     float* selfres = cs + 9 * L;                   // [kc][jc][P1M_MODES]
     const int* nbK = a.nb + (int64_t)K * a.N;
     const float* coefK = a.coef + (int64_t)K * 27 * L;
+    // Staging: the tables sit in L2, so its time is load latency.  Each thread
+    // issues a whole batch of loads into registers before its first shared
+    // store: 2 round trips for the φ rows, 1 for the pair coefficients and
+    // 1 for the self part (where a shared store after every load waited on
+    // each load in turn, 29 round trips).
     for (int il = threadIdx.x; il < L; il += blockDim.x) {
         const int sl = il / 3;
         const bool live = sl < cnt;
         const float* src = a.phi + (live ? (int64_t)(3 * nbK[sl] + il % 3) + (int64_t)a.n * (a.mode_lo + p0) : 0);
-#pragma unroll 8
-        for (int pp = 0; pp < P1M_MODES; ++pp)
-            phis[il * P1M_LD + pp] = (live && p0 + pp < a.M) ? src[(int64_t)a.n * pp] : 0.f;
+#pragma unroll
+        for (int h = 0; h < P1M_MODES; h += P1M_STAGE) {
+            float v[P1M_STAGE];
+#pragma unroll
+            for (int u = 0; u < P1M_STAGE; ++u)
+                v[u] = (live && p0 + h + u < a.M) ? src[(int64_t)a.n * (h + u)] : 0.f;
+#pragma unroll
+            for (int u = 0; u < P1M_STAGE; ++u) phis[il * P1M_LD + h + u] = v[u];
+        }
     }
-    for (int r = 0; r < 18; ++r) {                 // pair part: row r = kc·6 + t of the table
-        const int kc = r / 6, t = r - 6 * kc;
-        for (int j = threadIdx.x; j < L; j += blockDim.x) {
-            const int sl = j / 3, jc = j - 3 * sl;
-            const float c = coefK[r * L + j];
-            *reinterpret_cast<float2*>(cdup + ((sl * 9 + kc * 3 + jc) * 6 + t) * 2) = make_float2(c, c);
+    for (int j = threadIdx.x; j < L; j += blockDim.x) {   // pair part: row r = kc·6 + t of the table
+        const int sl = j / 3, jc = j - 3 * sl;
+        float c[18];
+#pragma unroll
+        for (int r = 0; r < 18; ++r) c[r] = coefK[r * L + j];
+#pragma unroll
+        for (int r = 0; r < 18; ++r) {
+            const int kc = r / 6, t = r - 6 * kc;
+            *reinterpret_cast<float2*>(cdup + ((sl * 9 + kc * 3 + jc) * 6 + t) * 2) = make_float2(c[r], c[r]);
         }
     }
     {
         const float4* cg = reinterpret_cast<const float4*>(coefK + 18 * L);
         float4* c4 = reinterpret_cast<float4*>(cs);
-        for (int e = threadIdx.x; e < 9 * L / 4; e += blockDim.x) c4[e] = cg[e];
+        const int E = 9 * L / 4;
+        for (int e0 = threadIdx.x; e0 < E; e0 += 4 * blockDim.x) {
+            float4 t[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = e0 + u * blockDim.x;
+                t[u] = e < E ? cg[e] : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (e0 + u * (int)blockDim.x < E) c4[e0 + u * blockDim.x] = t[u];
+        }
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
