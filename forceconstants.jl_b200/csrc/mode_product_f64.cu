@@ -118,11 +118,9 @@ int mode_product_f64(const double* A, const double* B, double* D, const ModeProd
     dim3 grid((unsigned)((mp.R + TM - 1) / TM), (unsigned)((mp.M + TN - 1) / TN));
     if (grid.y > 65535) return set_error(FCB_ERR_ARG, "mode product: too many modes");
     constexpr int smem = (int)sizeof(double) * 2 * TK * (TM + PAD + TN + PAD);
-    static bool attr = false;
-    if (!attr) {
-        FCB_CUDA(cudaFuncSetAttribute(mode_product_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr = true;
-    }
+    // a per-device attribute of the function: set on every launch, since
+    // handles on several devices may share this process
+    FCB_CUDA(cudaFuncSetAttribute(mode_product_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     mode_product_f64_kernel<<<grid, 256, smem, s>>>(A, B, D, mp);
     FCB_CUDA(cudaGetLastError());
     return FCB_OK;

@@ -1456,21 +1456,15 @@ int mode_product_tc(fcb200_context* h, int kind, const void* A_hi, const void* A
     }
     const int64_t tiles = (int64_t)p.m_tiles * p.n_tiles;
     const int grid = (int)(tiles < h->sm_count ? tiles : h->sm_count);
+    // The shared-memory limit is a per-device attribute of the function: set
+    // it on every launch (a handle per device may share this process).
     if (kind == 1) {
-        static bool attr = false;
-        if (!attr) {
-            FCB_CUDA(cudaFuncSetAttribute(mode_product_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          SMEM_BYTES));
-            attr = true;
-        }
+        FCB_CUDA(cudaFuncSetAttribute(mode_product_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      SMEM_BYTES));
         mode_product_tc_kernel<1><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(ma_hi, ma_lo, mb_hi, mb_lo, p);
     } else {
-        static bool attr = false;
-        if (!attr) {
-            FCB_CUDA(cudaFuncSetAttribute(mode_product_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          SMEM_BYTES));
-            attr = true;
-        }
+        FCB_CUDA(cudaFuncSetAttribute(mode_product_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      SMEM_BYTES));
         mode_product_tc_kernel<2><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(ma_hi, ma_lo, mb_hi, mb_lo, p);
     }
     FCB_CUDA(cudaGetLastError());
