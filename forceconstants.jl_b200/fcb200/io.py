@@ -8,10 +8,11 @@
 Text output keeps the reference's header, field order and loop order (1-based
 atom and component indices, only non-zero entries); floats are written in
 Julia's shortest round-trip form (``1.0e-5``, ``-0.0123``), so a file reads
-back bit for bit.  The reference's binary format is JLD2 (HDF5); no HDF5
-library is available to this package, so ``fmt="npz"`` stores the same keys
-(``F3``/``F2``, ``N_atoms``, ``dimension``, ``unit``) in a numpy archive
-instead, and ``fmt="JLD2"`` raises.
+back bit for bit.  The reference's default format, JLD2, is an HDF5 file with
+the keys ``F3``/``F2``, ``N_atoms``, ``dimension`` and ``unit``; ``fmt="JLD2"``
+(the default, as in the reference) writes that file through ``fcb200.hdf5``,
+and ``load_force_constants`` reads it back.  ``fmt="npz"`` stores the same
+keys in a numpy archive.
 """
 from __future__ import annotations
 
@@ -19,6 +20,7 @@ import os
 
 import numpy as np
 
+from . import hdf5
 from .arrays import is_torch
 from .types import DenseForceConstants
 
@@ -53,20 +55,25 @@ def _round_sig(x: float, digits: int = 7) -> float:
     return float(f"{x:.{digits - 1}e}") if x != 0.0 else 0.0
 
 
-def _check_out(outpath: str, filename: str, fmt: str, ext: dict) -> str:
-    if fmt not in ext:
-        raise ValueError(f"Invalid format, {fmt}" + (
-            " (JLD2 needs an HDF5 library; use fmt='npz')" if fmt.upper() == "JLD2" else ""))
-    return os.path.join(outpath, filename + ext[fmt])
+_EXT = {"txt": ".txt", "JLD2": ".jld2", "npz": ".npz"}
+
+
+def _check_out(outpath: str, filename: str, fmt: str) -> str:
+    if fmt not in _EXT:
+        raise ValueError(f"Invalid format, {fmt}")
+    return os.path.join(outpath, filename + _EXT[fmt])
 
 
 def save_third_order(psi, n_atoms: int, D: int, outpath: str, filename: str = "third_order",
-                     fmt: str = "txt") -> str:
+                     fmt: str = "JLD2") -> str:
     """io.jl:39-68.  Returns the path written."""
     v = _values(psi)
     n = n_atoms * D
     assert v.shape == (n, n, n), "Incorrect dimensions"
-    path = _check_out(outpath, filename, fmt, {"txt": ".txt", "npz": ".npz"})
+    path = _check_out(outpath, filename, fmt)
+    if fmt == "JLD2":
+        hdf5.write(path, {"F3": v, "N_atoms": int(n_atoms), "dimension": int(D), "unit": _units(psi, "")})
+        return path
     if fmt == "npz":
         np.savez(path, F3=np.asfortranarray(v), N_atoms=n_atoms, dimension=D, unit=_units(psi, ""))
         return path
@@ -86,12 +93,15 @@ def save_third_order(psi, n_atoms: int, D: int, outpath: str, filename: str = "t
 
 
 def save_second_order(phi, n_atoms: int, D: int, outpath: str, filename: str = "second_order",
-                      fmt: str = "txt") -> str:
+                      fmt: str = "JLD2") -> str:
     """io.jl:9-37.  Returns the path written."""
     v = _values(phi)
     n = n_atoms * D
     assert v.shape == (n, n), "Incorrect dimensions"
-    path = _check_out(outpath, filename, fmt, {"txt": ".txt", "npz": ".npz"})
+    path = _check_out(outpath, filename, fmt)
+    if fmt == "JLD2":
+        hdf5.write(path, {"F2": v, "N_atoms": int(n_atoms), "dimension": int(D), "unit": _units(phi, "")})
+        return path
     if fmt == "npz":
         np.savez(path, F2=np.asfortranarray(v), N_atoms=n_atoms, dimension=D, unit=_units(phi, ""))
         return path
@@ -119,6 +129,13 @@ def load_third_order_txt(path: str, n_atoms: int, D: int = 3) -> np.ndarray:
         ijk = rows[:, :6].astype(np.int64) - 1
         psi[D * ijk[:, 0] + ijk[:, 1], D * ijk[:, 2] + ijk[:, 3], D * ijk[:, 4] + ijk[:, 5]] = rows[:, 6]
     return psi
+
+
+def load_force_constants(path: str) -> dict:
+    """Reads a file written by save_third_order / save_second_order with
+    fmt="JLD2" (or any HDF5 file of plain datasets in its root group):
+    name -> value, arrays in Julia's column-major shape."""
+    return hdf5.read(path)
 
 
 def parse_xyz(path: str, n_atoms: int, n_steps: int):

@@ -1,7 +1,9 @@
 """Wire formats (fcb200.io) against the reference's io.jl: parse_xyz
 (io.jl:319-353) and save_third_order / save_second_order text output
-(io.jl:9-68) — header, 1-based fields, loop order, and a bit-exact read-back.
-CPU only."""
+(io.jl:9-68) — header, 1-based fields, loop order, and a bit-exact read-back —
+and the default JLD2 (HDF5) output: the checksum against its published test
+vectors, the reader against a file written by the HDF5 library, the writer's
+encodings against that file's, and bit-exact read-back.  CPU only."""
 import numpy as np
 import pytest
 
@@ -51,7 +53,7 @@ def test_save_third_order_txt(fcb, oracle, tmp_path):
     s, psi = _small_psi(oracle)
     N = s.n_atoms
     fc = fcb.DenseForceConstants(psi, "kcal mol^-1 Å^-3", 1e-12)
-    path = fcb.save_third_order(fc, N, 3, str(tmp_path))
+    path = fcb.save_third_order(fc, N, 3, str(tmp_path), fmt="txt")
     lines = open(path).read().splitlines()
     assert lines[0].startswith(f"#{N} atoms, Sum Ψ = ") and lines[0].endswith("Units: kcal mol^-1 Å^-3")
     body = [ln.split() for ln in lines[1:]]
@@ -69,7 +71,7 @@ def test_save_second_order_txt_and_npz(fcb, oracle, tmp_path):
     import fcb200 as f
     s = f.displaced(f.FCC(AR["a"], "Ar", (2, 2, 2)), 0.04, 9)
     ifc2 = oracle.second_order_lj(s.positions, s.box_sizes, AR["sigma"], AR["eps"], AR["r_cut"], 1e-12)
-    path = fcb.save_second_order(ifc2, s.n_atoms, 3, str(tmp_path))
+    path = fcb.save_second_order(ifc2, s.n_atoms, 3, str(tmp_path), fmt="txt")
     rows = np.loadtxt(path, comments="#")
     assert rows.shape[0] == np.count_nonzero(ifc2)
     got = np.zeros_like(ifc2)
@@ -84,9 +86,103 @@ def test_save_second_order_txt_and_npz(fcb, oracle, tmp_path):
 def test_formats_and_shapes_checked(fcb, oracle, tmp_path):
     s, psi = _small_psi(oracle)
     with pytest.raises(ValueError):
-        fcb.save_third_order(psi, s.n_atoms, 3, str(tmp_path), fmt="JLD2")
+        fcb.save_third_order(psi, s.n_atoms, 3, str(tmp_path), fmt="hdf5")
     with pytest.raises(AssertionError):
         fcb.save_third_order(psi, s.n_atoms + 1, 3, str(tmp_path))
     p = fcb.save_third_order(psi, s.n_atoms, 3, str(tmp_path), fmt="npz")
     z = np.load(p)
     assert np.array_equal(z["F3"], psi)
+
+
+# ---------------------------------------------------------------------------
+# JLD2 / HDF5
+
+def test_lookup3_published_vectors(fcb):
+    # the test values of Bob Jenkins' lookup3.c (hashlittle)
+    from fcb200.hdf5 import lookup3
+    assert lookup3(b"", 0) == 0xDEADBEEF
+    assert lookup3(b"", 0xDEADBEEF) == 0xBD5B7DDE
+    assert lookup3(b"Four score and seven years ago", 0) == 0x17770551
+    assert lookup3(b"Four score and seven years ago", 1) == 0xCD628161
+
+
+def _hdf5_library_file():
+    """A MAT 7.3 file (HDF5, written by the HDF5 library under MATLAB 7.4) from
+    scipy's test data, and the MAT 5 file holding the same variable."""
+    import os
+    scipy_io = pytest.importorskip("scipy.io")
+    data = os.path.join(os.path.dirname(scipy_io.matlab.__file__), "tests", "data")
+    h5, v5 = os.path.join(data, "testhdf5_7.4_GLNX86.mat"), os.path.join(data, "testdouble_7.4_GLNX86.mat")
+    if not (os.path.exists(h5) and os.path.exists(v5)):
+        pytest.skip("scipy's MAT test files are not installed")
+    return h5, v5
+
+
+def test_reader_on_a_file_written_by_the_hdf5_library(fcb):
+    # superblock 0 after a 512-byte user block, a symbol-table root group
+    # (B-tree, symbol-table node, local heap), version-1 object headers and a
+    # contiguous layout; the values must equal scipy's reading of the MAT 5
+    # file that holds the same variable
+    import scipy.io as sio
+    h5, v5 = _hdf5_library_file()
+    got = fcb.load_force_constants(h5)
+    ref = sio.loadmat(v5)["testdouble"]
+    assert set(got) == {"testdouble"}
+    assert got["testdouble"].shape == ref.shape == (1, 9)
+    assert np.array_equal(got["testdouble"], ref)
+
+
+def test_writer_encodings_match_the_hdf5_library(fcb, tmp_path):
+    # the float64 datatype message the writer emits is byte for byte the one
+    # the HDF5 library wrote for a MATLAB double
+    from fcb200 import hdf5
+    h5, _ = _hdf5_library_file()
+    lib = hdf5._File(open(h5, "rb").read())
+    addr = lib.links(lib.root)["testdouble"]
+    lib_dtype = [b for t, b in lib.messages(addr) if t == 0x03][0]
+    p = str(tmp_path / "x.jld2")
+    hdf5.write(p, {"x": np.zeros((2, 3))})
+    ours = hdf5._File(open(p, "rb").read())
+    our_dtype = [b for t, b in ours.messages(ours.links(ours.root)["x"]) if t == 0x03][0]
+    assert bytes(our_dtype) == bytes(lib_dtype[:len(our_dtype)])
+
+
+def test_save_third_order_jld2_default(fcb, oracle, tmp_path):
+    # the reference's default: jldsave(F3 = values, N_atoms, dimension, unit)
+    s, psi = _small_psi(oracle)
+    fc = fcb.DenseForceConstants(psi, "kcal mol^-1 Å^-3", 1e-12)
+    path = fcb.save_third_order(fc, s.n_atoms, 3, str(tmp_path))
+    assert path.endswith("third_order.jld2")
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"\x89HDF\r\n\x1a\n" and raw[8] == 2          # superblock version 2
+    got = fcb.load_force_constants(path)
+    assert set(got) == {"F3", "N_atoms", "dimension", "unit"}
+    assert got["F3"].shape == psi.shape and np.array_equal(got["F3"], psi)
+    assert got["N_atoms"] == s.n_atoms and got["dimension"] == 3
+    assert got["unit"] == "kcal mol^-1 Å^-3"
+    # every checksum is verified by the reader: a flipped byte in the root
+    # group header is reported
+    bad = bytearray(raw)
+    bad[60] ^= 0xFF
+    p2 = str(tmp_path / "bad.jld2")
+    open(p2, "wb").write(bytes(bad))
+    with pytest.raises(ValueError):
+        fcb.load_force_constants(p2)
+
+
+def test_save_second_order_jld2(fcb, oracle, tmp_path):
+    import fcb200 as f
+    s = f.displaced(f.FCC(AR["a"], "Ar", (2, 2, 2)), 0.04, 9)
+    ifc2 = oracle.second_order_lj(s.positions, s.box_sizes, AR["sigma"], AR["eps"], AR["r_cut"], 1e-12)
+    path = fcb.save_second_order(ifc2, s.n_atoms, 3, str(tmp_path), filename="phi")
+    got = fcb.load_force_constants(path)
+    assert path.endswith("phi.jld2") and np.array_equal(got["F2"], ifc2)
+    assert got["N_atoms"] == s.n_atoms and got["dimension"] == 3 and got["unit"] == ""
+    # a non-square (column-major) array keeps its Julia shape
+    a = np.asfortranarray(np.arange(24.0).reshape(2, 3, 4, order="F"))
+    from fcb200 import hdf5
+    p3 = str(tmp_path / "a.jld2")
+    hdf5.write(p3, {"a": a, "b": a.astype(np.float32)})
+    back = hdf5.read(p3)
+    assert back["a"].shape == (2, 3, 4) and np.array_equal(back["a"], a)
+    assert back["b"].dtype == np.float32 and np.array_equal(back["b"], a.astype(np.float32))
