@@ -352,6 +352,7 @@ int fcb200_third_order_lj(fcb200_handle h, const double* pos, int64_t N, const d
     if (!h) return set_error(FCB_ERR_ARG, "NULL handle");
     const bool weighted = (flags & FCB_PSI_MASS_WEIGHTED) != 0;
     FCB_TRY(validate_lj(pos, N, box, r_cut, masses, weighted || psi32_mw_out != nullptr));
+    if (!psi_out && !psi32_mw_out) return set_error(FCB_ERR_ARG, "no output buffer given");
     double bh[3];
     FCB_TRY(box_to_host(box, bh));
     FCB_TRY(check_cutoff(bh));

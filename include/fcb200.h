@@ -124,7 +124,8 @@ int fcb200_set_neighbour_capacity(fcb200_handle h, int cap);
  * psi_out   n³ doubles or NULL: Ψ after ASR and tol (mass weighted if flagged).
  * psi32_mw_out  n³ floats or NULL: FP32 copy of the mass-weighted Ψ.
  * Returns FCB_ERR_CUTOFF when r_cut >= a box length (the reference asserts
- * r_cut < L, third_order_analytical.jl:7).
+ * r_cut < L, third_order_analytical.jl:7), FCB_ERR_ARG when both outputs
+ * are NULL.
  */
 int fcb200_third_order_lj(fcb200_handle h, const double* pos, int64_t n_atoms, const double* box,
                           double sigma, double eps, double r_cut, double tol,
