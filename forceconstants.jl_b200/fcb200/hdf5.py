@@ -24,8 +24,9 @@ structures JLD2 itself uses:
 The reader handles these structures and the older ones the HDF5 library
 writes by default (superblock version 0, version-1 object headers,
 symbol-table groups with a version-1 B-tree, symbol-table nodes and a local
-heap; dataspace version 1, data layout versions 1-3), contiguous and compact
-datasets of integers, floats and fixed-length strings.  It is tested against
+heap; dataspace version 1, data layout versions 1-5), contiguous and compact
+datasets of integers, floats, fixed-length strings and JLD2's variable-length
+strings (global heap).  It is tested against
 a file written by the HDF5 library (and against the checksum's published test
 vectors); JLD2 and h5py are not available here, so files written by this
 module have been read back only by this reader.
@@ -401,9 +402,12 @@ class _File:
         count = int(np.prod(space)) if space else 1
         raw = self._data(layout, count * dtype[1])
         kind, size, np_dt = dtype
-        if kind == "s":
-            vals = [raw[i * size:(i + 1) * size].split(b"\x00", 1)[0].rstrip(b" ").decode("utf-8")
-                    for i in range(count)]
+        if kind in ("s", "vs"):
+            if kind == "s":
+                vals = [raw[i * size:(i + 1) * size].split(b"\x00", 1)[0].rstrip(b" ").decode("utf-8")
+                        for i in range(count)]
+            else:
+                vals = [self._vlen(raw[i * size:(i + 1) * size]).decode("utf-8") for i in range(count)]
             return vals[0] if not space else np.array(vals, dtype=object).reshape(tuple(reversed(space)), order="F")
         arr = np.frombuffer(raw, dtype=np_dt, count=count)
         if not space:
@@ -438,7 +442,30 @@ class _File:
             return "f", size, np.dtype(f"{order}f{size}")
         if cls == 3:
             return "s", size, None
+        if cls == 9 and (bits & 0x0F) == 1:   # variable-length string (JLD2's String)
+            return "vs", 16, None
         raise FormatError(f"datatype class {cls} is not read")
+
+    def _vlen(self, elem: bytes) -> bytes:
+        """A variable-length element: its length, then the global heap
+        collection's address and the object's index in it."""
+        length, coll, index = struct.unpack_from("<IQI", elem, 0)
+        if length == 0:
+            return b""
+        d = self.d
+        p = self.at(coll)
+        if d[p:p + 4] != b"GCOL":
+            raise FormatError("bad global heap collection")
+        end = p + struct.unpack_from("<Q", d, p + 8)[0]
+        q = p + 16
+        while q + 16 <= end:
+            idx, _refs, _res, size = struct.unpack_from("<HHIQ", d, q)
+            if idx == 0:
+                break
+            if idx == index:
+                return d[q + 16:q + 16 + min(length, size)]
+            q += 16 + (size + 7) // 8 * 8
+        raise FormatError("global heap object not found")
 
     def _data(self, body: bytes, nbytes: int) -> bytes:
         ver = body[0]
@@ -453,7 +480,7 @@ class _File:
                 size = struct.unpack_from("<I", body, p)[0]
                 return body[p + 4:p + 4 + min(size, nbytes)]
             raise FormatError("chunked layout is not read")
-        if ver == 3:
+        if ver in (3, 4, 5):                      # compact and contiguous are alike in 3-5
             cls = body[1]
             if cls == 0:
                 size = struct.unpack_from("<H", body, 2)[0]

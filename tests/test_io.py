@@ -186,3 +186,43 @@ def test_save_second_order_jld2(fcb, oracle, tmp_path):
     back = hdf5.read(p3)
     assert back["a"].shape == (2, 3, 4) and np.array_equal(back["a"], a)
     assert back["b"].dtype == np.float32 and np.array_equal(back["b"], a.astype(np.float32))
+
+
+def _vlen_string_file(path, name, text):
+    """A file holding one scalar variable-length UTF-8 string dataset, the
+    form JLD2 gives a String: the element (length, global heap collection
+    address, object index) points into a "GCOL" collection."""
+    import struct
+    from fcb200 import hdf5
+    payload = text.encode("utf-8")
+    gcol_addr, elem_addr = 512, 512 + 4096
+    obj = struct.pack("<HHIQ", 1, 1, 0, len(payload)) + payload + b"\x00" * (-len(payload) % 8)
+    free = struct.pack("<HHIQ", 0, 0, 0, 4096 - 16 - len(obj) - 16)
+    gcol = (b"GCOL" + bytes([1, 0, 0, 0]) + struct.pack("<Q", 4096) + obj + free).ljust(4096, b"\x00")
+    base_t = bytes([0x10, 0, 0, 0]) + struct.pack("<I", 1) + struct.pack("<HH", 0, 8)
+    vlen_t = bytes([0x19, 0x01, 0x01, 0x00]) + struct.pack("<I", 16) + base_t
+    ds = hdf5._object_header([hdf5._message(1, hdf5._dataspace(())), hdf5._message(3, vlen_t, 1),
+                              hdf5._message(5, hdf5._fill_value(), 1),
+                              hdf5._message(8, hdf5._layout_contiguous(elem_addr, 16))])
+    ds_addr = 256
+    nm = name.encode()
+    root = hdf5._object_header([hdf5._message(2, struct.pack("<BBQQ", 0, 0, hdf5.UNDEF, hdf5.UNDEF)),
+                                hdf5._message(10, struct.pack("<BB", 0, 0)),
+                                hdf5._message(6, struct.pack("<BBB", 1, 0, len(nm)) + nm + struct.pack("<Q", ds_addr))])
+    eof = elem_addr + 16
+    sb = hdf5.SIGNATURE + struct.pack("<BBBB", 2, 8, 8, 0) + struct.pack("<QQQQ", 0, hdf5.UNDEF, eof, 48)
+    out = bytearray(eof)
+    out[0:48] = sb + struct.pack("<I", hdf5.lookup3(sb))
+    out[48:48 + len(root)] = root
+    out[ds_addr:ds_addr + len(ds)] = ds
+    out[gcol_addr:gcol_addr + 4096] = gcol
+    out[elem_addr:elem_addr + 16] = struct.pack("<IQI", len(payload), gcol_addr, 1)
+    open(path, "wb").write(bytes(out))
+
+
+def test_reader_takes_variable_length_strings(fcb, tmp_path):
+    # the unit string of a file that JLD2 itself wrote is a variable-length
+    # string in the global heap
+    p = str(tmp_path / "v.jld2")
+    _vlen_string_file(p, "unit", "eV Å^-3")
+    assert fcb.load_force_constants(p) == {"unit": "eV Å^-3"}
