@@ -36,7 +36,7 @@ def build_oracle(force: bool = False) -> str:
 
 
 def build_reference_translation(reference_root: str | None = None, force: bool = False) -> str | None:
-    """Translate + compile the reference's generated SW derivative kernels.
+    """Translate + compile the reference's generated SW and LJ derivative kernels.
 
     ``reference_root`` (or the environment variable FCB200_REFERENCE_ROOT) is
     the ForceConstants.jl checkout; there is no default.  Returns the path of
@@ -55,7 +55,7 @@ def build_reference_translation(reference_root: str | None = None, force: bool =
     os.makedirs(REF_OUT, exist_ok=True)
     c_path = os.path.join(REF_OUT, "sw_generated.c")
     deps = [os.path.join(HERE, "sw_oracle.c"), os.path.join(HERE, "lj_oracle.c")]
-    if force or not os.path.exists(c_path):
+    if force or _stale(c_path, [os.path.join(HERE, "translate_sw_ref.py")]):
         translate_all(gen_dir, c_path)
     if force or _stale(lib, [c_path, *deps]):
         cmd = ["gcc", "-O1", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",

@@ -253,6 +253,91 @@ def second_order_lj(pos, box, sigma, eps, r_cut, tol):
     return ifc2.reshape((n, n), order="F")
 
 
+def _ref_lj_kernel(name):
+    L = ref_lib()
+    if L is None:
+        return None
+    f = getattr(L, name)
+    f.restype = None
+    f.argtypes = [_PD, _PD]
+    return f
+
+
+def _lj_pairs_ad(pos, box, r_cut):
+    """Pairs i < j within r_cut at the single minimum image, in the order of
+    the reference's loop (i ascending, then j), with r_ij = r_i - r_j mirrored
+    by nearest_mirror! (helper_funcs.jl:7-17)."""
+    pos, N = _pos(pos)
+    box = np.asarray(box, dtype=np.float64)
+    out = []
+    for i in range(N):
+        r = pos[i] - pos[i + 1:]
+        r = np.where(r > box / 2, r - box, np.where(r < -box / 2, r + box, r))
+        d2 = np.sum(r * r, axis=1)
+        for j in np.nonzero(d2 < r_cut * r_cut)[0]:
+            out.append((i, i + 1 + int(j), np.ascontiguousarray(r[j])))
+    return out, N
+
+
+def second_order_lj_ad_ref(pos, box, r_cut, tol):
+    """second_order! with the AutoDiffCalculator for LJ
+    (src/autodiff/second_order_AD.jl:1-37) driven by the reference's own
+    generated Hessian kernel (H2_exec_LJ, σ = 3.4 Å and ϵ = 0.24037 kcal/mol
+    baked in), then ASR! (asr.jl:3-17) and apply_tols! (ifc.jl:12).  None when
+    oracle/_ref is not built."""
+    h2 = _ref_lj_kernel("ref_H2_exec_LJ")
+    if h2 is None:
+        return None
+    pairs, N = _lj_pairs_ad(pos, box, r_cut)
+    n = 3 * N
+    ifc2 = np.zeros((n, n), order="F")
+    blk = np.zeros(9)
+    for i, j, r in pairs:
+        h2(_pd(r), _pd(blk))
+        b = -blk.reshape((3, 3), order="F")
+        ifc2[3 * i:3 * i + 3, 3 * j:3 * j + 3] = b
+        ifc2[3 * j:3 * j + 3, 3 * i:3 * i + 3] = b
+    for i in range(N):
+        for a in range(3):
+            for c in range(3):
+                ifc2[3 * i + a, 3 * i + c] = -np.sum(ifc2[3 * i + a, c::3])
+    ifc2[np.abs(ifc2) < tol] = 0.0
+    return ifc2
+
+
+def third_order_lj_ad_ref(pos, box, r_cut, tol):
+    """third_order! with the AutoDiffCalculator for LJ
+    (src/autodiff/third_order_AD.jl:1-69) driven by the reference's own
+    generated third-derivative kernel (H3_exec_LJ): per pair i < j the block
+    -H3(r_ij) is assigned at (i,i,j), (i,j,i), (j,i,i) and its negative at
+    (i,j,j), (j,j,i), (j,i,j); then ASR! (asr.jl:19-40: every (iα, jβ, iγ)
+    becomes minus the sum of its row over the third index) and apply_tols!
+    (ifc.jl:30).  None when oracle/_ref is not built."""
+    h3 = _ref_lj_kernel("ref_H3_exec_LJ")
+    if h3 is None:
+        return None
+    pairs, N = _lj_pairs_ad(pos, box, r_cut)
+    n = 3 * N
+    psi = np.zeros((n, n, n), order="F")
+    blk = np.zeros(27)
+    for i, j, r in pairs:
+        h3(_pd(r), _pd(blk))
+        b = -blk.reshape((3, 3, 3), order="F")
+        I, J = slice(3 * i, 3 * i + 3), slice(3 * j, 3 * j + 3)
+        psi[I, I, J] = b
+        psi[I, J, I] = b
+        psi[J, I, I] = b
+        psi[I, J, J] = -b
+        psi[J, J, I] = -b
+        psi[J, I, J] = -b
+    six = psi.reshape((3, N, 3, N, 3, N), order="F")
+    for i in range(N):
+        six[:, i, :, :, :, i] = 0.0
+        six[:, i, :, :, :, i] = -np.sum(six[:, i, :, :, :, :], axis=4)
+    psi[np.abs(psi) < tol] = 0.0
+    return psi
+
+
 def mass_weight_third_order(psi, masses):
     """third_order_analytical.jl:185-214, in place on a Fortran-ordered array."""
     assert psi.flags.f_contiguous and psi.dtype == np.float64

@@ -14,6 +14,10 @@ Inputs (relative to the reference root):
   ``var"##n" = a op b`` and ``result[CartesianIndex(a,b,c)] = v``.
   Used by ``third_order!``/``second_order!`` for SW
   (``src/autodiff/third_order_AD.jl:71-170``, ``second_order_AD.jl:40-110``).
+* ``LJ/H2_exec_LJ.jl``, ``LJ/H3_exec_LJ.jl`` — FastDifferentiation output for
+  the LJ pair (σ and ϵ of the reference's tests baked in), used by
+  ``second_order!``/``third_order!`` with the AutoDiffCalculator
+  (``second_order_AD.jl:1-37``, ``third_order_AD.jl:1-69``).
 * ``SW_sym_iik/H3_exec_iik_{abc}.jl`` — Symbolics output, one prefix-form
   expression per component of the iik block.  The reference builds this block
   at run time with Symbolics from ``three_body_potential_nounits`` using the
@@ -202,6 +206,10 @@ def translate_all(gen_dir: str, out_c: str) -> None:
                 comps.append(((a - 1) + 3 * (b - 1) + 9 * (c - 1), name))
     parts.append("void ref_H3_exec_iik(const double* x, double* out) {\n" +
                  "\n".join(f"    out[{f}] = {n}(x);" for f, n in comps) + "\n}\n")
+    # LJ pair blocks of the AutoDiffCalculator (σ = 3.4 Å, ϵ = 0.24037 kcal/mol
+    # baked in): second_order_AD.jl:25, third_order_AD.jl:26
+    parts.append(translate_fd(os.path.join(gen_dir, "LJ", "H2_exec_LJ.jl"), "ref_H2_exec_LJ"))
+    parts.append(translate_fd(os.path.join(gen_dir, "LJ", "H3_exec_LJ.jl"), "ref_H3_exec_LJ"))
     os.makedirs(os.path.dirname(out_c), exist_ok=True)
     with open(out_c, "w") as f:
         f.write("\n".join(parts))

@@ -54,6 +54,10 @@ def main(reference_root: str) -> None:
         sys.path.insert(0, HERE)
         import make_sw_golden  # noqa: E402
         make_sw_golden.main(reference_root)
+    if os.path.exists(os.path.join(HERE, "make_lj_ad_golden.py")):
+        sys.path.insert(0, HERE)
+        import make_lj_ad_golden  # noqa: E402
+        make_lj_ad_golden.main(reference_root)
 
 
 if __name__ == "__main__":

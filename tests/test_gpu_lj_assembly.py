@@ -134,3 +134,24 @@ def test_deterministic_repeat(fcb, cuda_device):
     a = _cpu(fcb.third_order(s, pot, calc, device="cuda").values)
     b = _cpu(fcb.third_order(s, pot, calc, device="cuda").values)
     assert np.array_equal(a, b)
+
+
+def test_autodiff_calculator_vs_reference_ad_golden(fcb, cuda_device):
+    # The reference's "LJ AD vs Analytical" set (test/runtests.jl:139-162)
+    # through the public API: third_order / second_order with the
+    # AutoDiffCalculator (answered by the analytical kernels) against the
+    # result of the reference's own AD kernels (H3_exec_LJ / H2_exec_LJ driven
+    # by third_order_AD.jl:1-69 and second_order_AD.jl:1-37), within the
+    # reference's atol of 1e-12 on the whole array (Frobenius norm).
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "lj_ad_fcc_2x2x2_std0.05_seed3.npz"))
+    s = fcb.SuperCellSystem(d["positions"], np.full(len(d["positions"]), AR["mass"]), d["box"])
+    pot = fcb.LJ(float(d["sigma"]), float(d["eps"]), float(d["r_cut"]))
+    calc = fcb.AutoDiffCalculator(float(d["tol"]), float(d["r_cut"]))
+    n = int(d["n"])
+    flat = np.zeros(n ** 3)
+    flat[d["ifc3_index"]] = d["ifc3_value"]
+    ref3 = flat.reshape((n, n, n), order="F")
+    got3 = _cpu(fcb.third_order(s, pot, calc, device="cuda").values)
+    assert np.linalg.norm((got3 - ref3).ravel()) <= 1e-12
+    got2 = _cpu(fcb.second_order(s, pot, calc, device="cuda").values)
+    assert np.linalg.norm((got2 - d["ifc2"]).ravel()) <= 1e-12
