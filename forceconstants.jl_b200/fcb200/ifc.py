@@ -49,7 +49,9 @@ def third_order_(psi, sys: SuperCellSystem, pot, calc, n_threads: int | None = N
     n = 3 * sys.n_atoms
     if tuple(psi.shape) != (n, n, n):
         raise AssertionError("size(Ψ) == (D*N_atoms, D*N_atoms, D*N_atoms)")
-    _check_cut(sys, calc.r_cut)
+    if isinstance(calc, AnalyticalCalculator):
+        _check_cut(sys, pot.r_cut)      # the reference asserts on the potential's cutoff
+    _check_cut(sys, calc.r_cut)         # the pair loop's single minimum image needs r_cut < L
     m = sys.masses if masses is None else np.ascontiguousarray(masses, dtype=np.float64)
     need_m = mass_weighted or psi32_mw is not None
     flags = _lib.FCB_PSI_MASS_WEIGHTED if mass_weighted else 0
@@ -105,6 +107,9 @@ def second_order_(ifc2, sys: SuperCellSystem, pot, calc, n_threads: int | None =
         return second_order_sw_(ifc2, sys, pot, calc, masses=masses)
     if not isinstance(pot, LJ):
         raise TypeError(f"no second_order! method for {type(pot).__name__}")
+    if isinstance(calc, AutoDiffCalculator) and not calc.r_cut <= pot.r_cut:
+        # second_order_AD.jl:4
+        raise AssertionError("Calculator r_cut must be less than potential r_cut")
     dev = device_index(ifc2)
     m = None if masses is None else np.ascontiguousarray(masses, dtype=np.float64)
     _lib.check(_lib.lib().fcb200_second_order_lj(

@@ -38,6 +38,16 @@ def test_cutoff_assertion_before_any_device_work(fcb):
     psi = np.zeros((12, 12, 12), order="F")
     with pytest.raises(AssertionError, match="Cutoff"):
         fcb.third_order_(psi, s, pot, calc)
+    # third_order_analytical.jl:7 asserts on the potential's cutoff, even when
+    # the calculator's is shorter
+    s2 = fcc_system((2, 2, 2))
+    psi2 = np.zeros((96, 96, 96), order="F")
+    with pytest.raises(AssertionError, match="Cutoff"):
+        fcb.third_order_(psi2, s2, fcb.LJ(AR["sigma"], AR["eps"], 11.0), calc)
+    # second_order_AD.jl:4: the AutoDiffCalculator's cutoff may not exceed the potential's
+    with pytest.raises(AssertionError, match="Calculator r_cut"):
+        fcb.second_order_(np.zeros((96, 96), order="F"), s2, fcb.LJ(AR["sigma"], AR["eps"], 8.0),
+                          fcb.AutoDiffCalculator(1e-12, AR["r_cut"]))
 
 
 def test_julia_layout_helpers(fcb):
