@@ -140,18 +140,36 @@ def load_force_constants(path: str) -> dict:
 
 def parse_xyz(path: str, n_atoms: int, n_steps: int):
     """io.jl:319-353: frames of two header lines followed by n_atoms lines
-    `id x y z`.  Returns (positions, ids): positions[s] is an (n_atoms, 3)
-    float64 array and ids[s] the atom ids of frame s, for s < n_steps; frames
-    past n_steps are ignored and missing frames come back empty, as the
-    reference's pre-sized vectors do."""
-    positions = [np.empty((0, 3)) for _ in range(n_steps)]
-    ids = [np.empty((0,), dtype=np.int64) for _ in range(n_steps)]
+    `id x y z`.  Returns (positions, ids): positions[s] is a (k, 3) float64
+    array (every column after the id, as the reference's `posn...`) and ids[s]
+    the atom ids of frame s, for s < n_steps.  The reference's state machine
+    is kept: blank lines are skipped (readdlm), a frame the file does not hold
+    comes back empty and a truncated last frame with the atoms it has, and an
+    atom line past frame n_steps raises IndexError (Julia's BoundsError), as
+    does an id that is not an integer raise ValueError (InexactError)."""
+    rows = [[] for _ in range(n_steps)]
+    ids = [[] for _ in range(n_steps)]
+    header_size = 2
+    line_num = 0
+    step = 0
     with open(path) as f:
-        lines = f.read().splitlines()
-    frame = n_atoms + 2
-    for s in range(min(n_steps, len(lines) // frame)):
-        body = lines[s * frame + 2:(s + 1) * frame]
-        arr = np.array([ln.split() for ln in body], dtype=np.float64)
-        ids[s] = arr[:, 0].astype(np.int64)
-        positions[s] = np.ascontiguousarray(arr[:, 1:4])
-    return positions, ids
+        for raw in f:
+            tok = raw.split()
+            if not tok:
+                continue
+            if line_num in (0, 1):
+                line_num += 1
+                continue
+            if step >= n_steps:
+                raise IndexError(f"attempt to access {n_steps}-element Vector at index [{step + 1}]")
+            idv = float(tok[0])
+            if not idv.is_integer():
+                raise ValueError(f"InexactError: Int64({tok[0]})")
+            ids[step].append(int(idv))
+            rows[step].append([float(x) for x in tok[1:]])
+            line_num += 1
+            if line_num == n_atoms + header_size:
+                line_num = 0
+                step += 1
+    positions = [np.array(r, dtype=np.float64).reshape(len(r), -1) if r else np.empty((0, 3)) for r in rows]
+    return positions, [np.array(i, dtype=np.int64) for i in ids]

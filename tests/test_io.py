@@ -39,6 +39,23 @@ def test_parse_xyz(fcb, tmp_path):
     # asking for more frames than the file holds leaves the extra ones empty
     pos2, ids2 = fcb.parse_xyz(str(p), n_atoms, steps + 2)
     assert pos2[-1].shape == (0, 3) and ids2[-1].shape == (0,)
+    # fewer frames than the file holds: the reference's push! into frame
+    # n_steps + 1 is a BoundsError
+    with pytest.raises(IndexError):
+        fcb.parse_xyz(str(p), n_atoms, steps - 1)
+    # blank lines are skipped (readdlm) and a truncated last frame keeps the
+    # atoms it has
+    q = tmp_path / "cut.xyz"
+    with open(q, "w") as f:
+        f.write(f"{n_atoms}\nstep 0\n\n")
+        for a, x in enumerate(frames[0]):
+            f.write(f"{a + 1} {float(x[0])!r} {float(x[1])!r} {float(x[2])!r}\n")
+        f.write(f"{n_atoms}\nstep 1\n")
+        for a, x in enumerate(frames[1][:2]):
+            f.write(f"{a + 1} {float(x[0])!r} {float(x[1])!r} {float(x[2])!r}\n")
+    pos3, ids3 = fcb.parse_xyz(str(q), n_atoms, 2)
+    assert np.array_equal(pos3[0], frames[0]) and np.array_equal(pos3[1], frames[1][:2])
+    assert list(ids3[1]) == [1, 2]
     # a frame of the trajectory is a snapshot the library takes as positions
     assert pos[1].reshape(-1).shape == (3 * n_atoms,)
 
