@@ -368,14 +368,12 @@ class _File:
         while stack:
             p = self.at(stack.pop())
             if d[p:p + 4] == b"TREE":
-                ntype, level, used = d[p + 4], d[p + 5], struct.unpack_from("<H", d, p + 6)[0]
+                ntype, used = d[p + 4], struct.unpack_from("<H", d, p + 6)[0]
                 if ntype != 0:
                     raise FormatError("not a group B-tree")
                 q = p + 24 + 8                            # past the siblings and key 0
-                for _ in range(used):
-                    stack.append(self.q(q))
-                    q += 16
-                del level
+                children = [self.q(q + 16 * c) for c in range(used)]
+                stack.extend(reversed(children))          # visited in key (name) order
             elif d[p:p + 4] == b"SNOD":
                 nsym = struct.unpack_from("<H", d, p + 6)[0]
                 q = p + 8
@@ -416,7 +414,7 @@ class _File:
 
     @staticmethod
     def _dataspace(body: bytes) -> tuple[int, ...]:
-        ver, rank, flags = body[0], body[1], body[2]
+        ver, rank = body[0], body[1]
         if ver == 1:
             p = 8
         elif ver == 2:
@@ -425,7 +423,6 @@ class _File:
             p = 4
         else:
             raise FormatError(f"dataspace version {ver}")
-        del flags
         return tuple(struct.unpack_from("<Q", body, p + 8 * i)[0] for i in range(rank))
 
     @staticmethod
